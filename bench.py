@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Kirchhoff post-stack 3D time migration.
+
+One step = one forward migration (diffraction summation) of the whole resident cube of the
+production workload: 401x401 traces x 1001 samples at 2 ms, 25 m bins, Vrms 1500->3500 m/s
+with a 5% lateral Gaussian perturbation, 45 deg aperture, amplitude correction on (seeded
+synthetic data, poststackmig3d_b200.synth.workload_config2).
+
+metric: summed input samples/s (G/s) = (output sample, input trace) terms that pass every
+mask of the reference, counted exactly by psm_count_terms, per second.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU implementation of the path
+(MigrationKernel::kirchhoffKernel3DWithPadding compiled from its sources into oracle/_ref,
+OpenMP on all host cores) on a bounded sample of output inlines of the same workload.
+Multi-GPU (torchrun): independent replicas, one per GPU, no collective on the data path
+(weak scaling); value = all ranks' terms / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("summed input samples/s (G/s) on 1 B200, mixed/batched vs plain FP32 at stated "
+          "rel err")
+UNIT = "G/s"
+# Per-term limb budget of the summation on one SM per clock: 16 SFU (MUFU) ops, 128 FP32
+# lanes / ~8 FP32 ops, 32 shared-memory words / 2 samples -> 16 terms/clk/SM for each limb.
+TERMS_PER_CLK_SM = 16.0
+N_SM = 148
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["config2", "config1"], default="config2")
+    p.add_argument("--cpu-rows", type=int, default=2,
+                   help="output inlines in the bounded CPU sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(name):
+    from poststackmig3d_b200 import synth as S
+    return S.workload_config2() if name == "config2" else S.workload_config1()
+
+
+def geometry(W):
+    from poststackmig3d_b200 import estimate_max_velocity, plan_geometry
+    n_il, n_xl, n_t = W.data.shape
+    return plan_geometry(n_il, n_xl, n_t, W.dt, W.d_il, W.d_xl, W.angle,
+                         estimate_max_velocity(W.vrms_cube()), W.pad_il, W.pad_xl, W.amp)
+
+
+def config_dict(W, g, extra=None):
+    d = {"workload": f"{W.name}: {g.n_il}x{g.n_xl} traces x {g.n_t} samples, "
+                     f"dt {g.dt_seconds * 1e3:.0f} ms, {W.d_il:.0f} m bins, "
+                     f"{W.angle:.0f} deg aperture, amp {'on' if W.amp else 'off'}, "
+                     f"pad {W.pad_il}/{W.pad_xl}",
+         "traces": [g.n_il, g.n_xl], "samples": g.n_t, "image": [g.n_oi, g.n_ox, g.n_t],
+         "m_il": g.m_il, "storage": "f32",
+         "l2": "inputs larger than L2 (cube 644 MB, Vrms 644 MB)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# --------------------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock, power and throttle reasons."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.rows = []
+        self.proc = None
+        self.t = None
+        self.device_id = device_id
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", self.device_id], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.t:
+            self.t.join(timeout=5)
+
+    def summary(self):
+        sm = []
+        mx = []
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def profile_traffic():
+    """DRAM bytes per forward launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "fwd_kernel_config2.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":")[1].split()[0])
+            except (IndexError, ValueError):
+                return None
+    return None
+
+
+# --------------------------------------------------------------------------- CPU arm
+
+
+def cpu_reference_sample(W, g, rows, threads):
+    """Time the reference's own kirchhoffKernel3DWithPadding (oracle/_ref, OpenMP build, all
+    host threads) on output inlines `rows`, with the buffers its driver would prepare
+    (prepareInputBufferWithPadding / prepareVelocitySliceWithPadding).  Falls back to the
+    oracle port when the reference was not built.  Returns (terms, seconds, kind)."""
+    import oracle as O
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    n_il, n_xl, n_t = W.data.shape
+    t0 = g.t0()
+    vr = W.vrms_cube()
+    terms = 0
+    secs = 0.0
+    kind = "reference" if O.ref_available() else "port"
+    for r in rows:
+        c = int(g.out_center[r])
+        rs, re = max(0, c - g.m_il), min(n_il, c + g.m_il + 1)
+        il0, il1 = max(0, rs - g.pad_il), min(n_il, re + g.pad_il)
+        nbx = n_xl + 2 * g.pad_xl
+        if g.pad_xl:
+            buf = np.zeros((il1 - il0, nbx, n_t), dtype=np.float32)
+            buf[:, g.pad_xl:g.pad_xl + n_xl] = W.data[il0:il1]
+            vel = np.zeros((nbx, n_t), dtype=np.float32)
+            vel[g.pad_xl:g.pad_xl + n_xl] = vr[c]
+        else:
+            buf = W.data[il0:il1]
+            vel = vr[c]
+        il_pos = np.arange(il0, il1, dtype=np.int32)
+        cnt = O.count_rows(vr, g.out_center, r, r + 1, g.n_ox, g.pad_il, g.pad_xl, g.m_il,
+                           np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il, g.d_xl,
+                           g.amp, threads=threads)
+        terms += int(cnt[0])
+        t = time.perf_counter()
+        if kind == "reference":
+            O.ref_kirchhoff_inline(buf, vel, g.n_ox, il_pos, c - il0, 0,
+                                   np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il,
+                                   g.d_xl, g.amp, kind="omp")
+        else:
+            O.kirchhoff_inline(buf, vel, g.n_ox, il_pos, c - il0, 0,
+                               np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il,
+                               g.d_xl, g.amp)
+        secs += time.perf_counter() - t
+    return terms, secs, kind
+
+
+def sample_rows(g, k):
+    mid = g.n_oi // 2
+    return [min(g.n_oi - 1, mid + i) for i in range(k)]
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    W = workload(args.workload)
+    g = geometry(W)
+    rows = sample_rows(g, args.cpu_rows)
+    vals = []
+    kind = "reference"
+    for i in range(args.warmup + args.steps):
+        terms, secs, kind = cpu_reference_sample(W, g, rows, threads)
+        if i >= args.warmup:
+            vals.append((terms, secs))
+    terms = sum(v[0] for v in vals)
+    secs = sum(v[1] for v in vals)
+    value = terms / secs / 1e9
+    sample = (f"{len(rows)} central output inlines of {W.name} per step "
+              f"(rows {rows[0]}..{rows[-1]}, {terms // max(len(vals), 1)} terms/step)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": secs / max(len(vals), 1) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": config_dict(W, g),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- GPU arm
+
+
+def run_ours(args):
+    import torch
+    from poststackmig3d_b200 import Migrator
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    W = workload(args.workload)
+    g = geometry(W)
+    m = Migrator(local)
+    m.set_geometry(g)
+    m.set_traces(W.data)
+    m.set_vrms(W.vrms_cube())
+    n_terms = m.count_terms()
+    stream = torch.cuda.ExternalStream(m.stream_handle())
+
+    for _ in range(max(args.warmup, 0)):
+        m.forward_async()
+    m.synchronize()
+
+    props = torch.cuda.get_device_properties(local)
+    uuid = str(getattr(props, "uuid", ""))
+    dev_id = ("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or str(local))
+    clk = ClockSampler(dev_id)
+
+    # ---- device-resident throughput: K forward launches between two events
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    time.sleep(0.25)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        m.forward_async()
+    ev1.record(stream)
+    m.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clk.stop()
+    if dist:
+        dist.barrier()
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * n_terms / (ms_max * 1e-3) / 1e9
+
+    # ---- end to end through the public API: pinned host inputs -> image on the host
+    h_data = torch.from_numpy(W.data).pin_memory()
+    h_vrms = torch.from_numpy(W.vrms_cube()).pin_memory()
+    h_img = torch.empty(m.image_shape(), dtype=torch.float32).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    m.set_traces(h_data)
+    m.set_vrms(h_vrms)
+    m.forward(h_img)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        m.set_traces(h_data)
+        m.set_vrms(h_vrms)
+        m.forward(h_img)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n_terms / (e2e_ms * 1e-3) / 1e9
+
+    clocks = clk.summary()
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    peak = TERMS_PER_CLK_SM * N_SM * sm_mhz * 1e6 / 1e9  # Gterm/s
+    achieved = n_terms / (ms * 1e-3) / 1e9
+    comp_bytes = (2 * g.n_il * g.n_xl * g.n_t + g.n_oi * g.n_ox * g.n_t) * 4
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm_peak = float(peaks["hbm_gbs"])
+        hbm_src = "measured"
+    except Exception:
+        hbm_peak, hbm_src = 6650.0, "fallback"
+    hbm_ach = comp_bytes / (ms * 1e-3) / 1e9
+    roofline = {
+        "bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gterm/s",
+        "frac": achieved / peak, "traffic": profile_traffic(),
+        "peak_basis": f"{TERMS_PER_CLK_SM:.0f} terms/clk/SM (SFU, FP32, LDS limbs) x {N_SM} "
+                      f"SMs x median SM clock {sm_mhz:.0f} MHz under load",
+        "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": hbm_ach / hbm_peak, "peak_source": hbm_src,
+                "algorithmic_bytes_per_launch": comp_bytes},
+    }
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rows = sample_rows(g, args.cpu_rows)
+        terms, secs, kind = cpu_reference_sample(W, g, rows, threads)
+        cpu = {"value": terms / secs / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{len(rows)} central output inlines of {W.name} "
+                         f"({terms} terms, {secs:.1f} s)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded)",
+                "config": config_dict(W, g, {"n_terms": n_terms,
+                                             "parallelism": f"replicas x{world}"}),
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT,
+                        "h2d_bytes_per_step": int(h_data.numel() * 4 + h_vrms.numel() * 4),
+                        "d2h_bytes_per_step": int(h_img.numel() * 4)},
+                "gpu_launches": args.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    m.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,130 @@
+/* psm.h -- C ABI of libpsm_cuda.so, the B200 (sm_100a) Kirchhoff post-stack 3D time
+ * migration.
+ *
+ * The reference (sergeevsn/poststackmig3d) has no FFI; its seam is the static C++ class
+ * MigrationKernel (include/migration_kernel.h:11-74), called from src/main.cpp:298, :314 and
+ * :357.  The entry points below replace that seam.  Every function returns PSM_OK (0) or a
+ * negative psm_status; no C++ exception crosses this boundary.  Host pointers are owned by
+ * the caller; device memory allocated by the library is owned by the psm_ctx.  A psm_ctx is
+ * bound to one device and one CUDA stream and is not thread-safe (one per host thread).
+ * Calls return when their work is complete unless the name ends in _async.
+ */
+#ifndef PSM_H
+#define PSM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PSM_OK = 0,
+    PSM_ERR_ARG = -1,        /* invalid argument / size */
+    PSM_ERR_STATE = -2,      /* call out of order (e.g. forward before set_traces) */
+    PSM_ERR_CUDA = -3,       /* a CUDA runtime call failed */
+    PSM_ERR_NOMEM = -4,      /* device allocation failed */
+    PSM_ERR_DEVICE = -5,     /* a kernel reported an error (bounded wait expired, ...) */
+    PSM_ERR_UNSUPPORTED = -6 /* size or mode outside what the kernels handle */
+} psm_status;
+
+typedef enum { PSM_F32 = 0, PSM_BF16 = 1, PSM_F16 = 2 } psm_precision;
+
+/* Geometry and migration parameters of a resident cube.  The values are the ones the
+ * reference driver derives (src/main.cpp:124-217):
+ *   n_il, n_xl, n_t   real input grid (sorted unique inline / crossline labels, samples)
+ *   dt                sample interval in seconds, as float (main.cpp:363)
+ *   dt_seconds        the same interval in double; t0[i] = float(i * dt_seconds)
+ *                     (main.cpp:214-217)
+ *   d_il, d_xl        inline_step / crossline_step in metres
+ *   tan2_theta        float(tan(angle)) squared (main.cpp:188-189)
+ *   m_il              inline aperture of the buffer (main.cpp:201)
+ *   pad_il, pad_xl    inline_padding / crossline_padding
+ *   n_oi, n_ox        output inlines / crosslines (labels padded by main.cpp:144-172)
+ *   amp_correction    1/(t v^2) weighting on/off
+ *   precision         storage of the traces in HBM (psm_precision)
+ */
+typedef struct {
+    int32_t n_il, n_xl, n_t;
+    int32_t pad_il, pad_xl;
+    int32_t n_oi, n_ox;
+    int32_t m_il;
+    int32_t amp_correction;
+    int32_t precision;
+    float dt;
+    float d_il, d_xl;
+    float tan2_theta;
+    double dt_seconds;
+} psm_geom;
+
+typedef struct psm_ctx psm_ctx;
+
+/* Library / device. */
+const char *psm_version(void);
+int psm_device_count(int *count);
+
+/* Context lifetime: one GPU, one stream. */
+int psm_create(psm_ctx **out, int device);
+int psm_destroy(psm_ctx *ctx);
+const char *psm_last_error(const psm_ctx *ctx); /* message of the last failure on ctx */
+
+/* Geometry.  out_center[n_oi] gives, for every output inline, the real inline index it
+ * migrates (main.cpp:258-288: padded output inlines take the nearest real inline); NULL
+ * means the regular-label rule clamp(o - pad_il, 0, n_il - 1).  Replaces the per-inline
+ * buffer set-up of MigrationKernel::prepareInputBufferWithPadding
+ * (src/migration_kernel.cpp:385-468): the whole cube stays resident in HBM. */
+int psm_set_geometry(psm_ctx *ctx, const psm_geom *g, const int32_t *out_center);
+
+/* Upload the traces [n_il][n_xl][n_t] (host, float32, real grid, missing traces zero).
+ * Replaces the per-inline re-reads of prepareInputBufferWithPadding. */
+int psm_set_traces(psm_ctx *ctx, const float *data);
+
+/* Upload the Vrms cube [n_il][n_xl][n_t] of the output points (host, float32).  Replaces
+ * MigrationKernel::prepareVelocitySliceWithPadding (src/migration_kernel.cpp:470-511);
+ * padded crosslines get v = 0 inside the kernel. */
+int psm_set_vrms(psm_ctx *ctx, const float *vrms);
+
+/* Forward operator (migration, diffraction summation) of the whole resident cube into
+ * image[n_oi][n_ox][n_t] (host).  This is kirchhoffKernel3DWithPadding
+ * (src/migration_kernel.cpp:17-383) applied to every output inline of src/main.cpp:257-369. */
+int psm_forward(psm_ctx *ctx, float *image);
+
+/* Same, leaving the image in device memory owned by ctx (enqueued on the ctx stream). */
+int psm_forward_async(psm_ctx *ctx);
+int psm_synchronize(psm_ctx *ctx);
+/* Device pointer of the ctx-owned image [n_oi][n_ox][n_t] (valid until the next
+ * psm_set_geometry / psm_destroy). */
+int psm_image_device(psm_ctx *ctx, float **dev_image);
+/* Copy the ctx-owned image to the host. */
+int psm_get_image(psm_ctx *ctx, float *image);
+/* Raw CUDA stream of the ctx (a cudaStream_t). */
+int psm_stream(psm_ctx *ctx, void **stream);
+
+/* Number of (output sample, input trace) terms that pass every mask of the reference
+ * (migration_kernel.cpp:166, :207/:286, :226/:298) over the real input traces, counted on
+ * the GPU with the forward kernel's own arithmetic. */
+int psm_count_terms(psm_ctx *ctx, int64_t *n_terms);
+/* The same count per output inline: per_row[n_oi]. */
+int psm_count_terms_rows(psm_ctx *ctx, int64_t *per_row);
+
+/* Per-inline drop-in for MigrationKernel::kirchhoffKernel3DWithPadding
+ * (include/migration_kernel.h:16-31, src/migration_kernel.cpp:17-383): the same arguments,
+ * output_slice flat [n_out_xl][n_t] instead of vector<vector<float>>; xl_pos_indices is
+ * unused (as in the reference) and may be NULL.  Uploads the buffer on each call, so it is
+ * the slow path; the resident-cube calls above are the fast path.  Thread-safe: each host
+ * thread gets its own device staging. */
+int psm_kirchhoff_inline(const float *input_buffer, size_t n_buf_il, size_t n_buf_xl,
+                         size_t n_t, const float *velocity_slice, float *output_slice,
+                         size_t n_out_xl, const int32_t *il_pos_indices,
+                         const int32_t *xl_pos_indices, int32_t current_il_pos,
+                         int32_t current_xl_start, float dt, const float *t0_times,
+                         float tan_theta_sq, float inline_bin_size,
+                         float crossline_bin_size, int amp_correction);
+/* Message of the last psm_kirchhoff_inline failure on this thread. */
+const char *psm_kirchhoff_inline_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSM_H */

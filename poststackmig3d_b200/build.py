@@ -1,0 +1,79 @@
+"""Build recipe for the native parts of poststackmig3d_b200 (in-tree, no JIT cache).
+
+    python -m poststackmig3d_b200.build
+
+produces
+    poststackmig3d_b200/lib/libpsm_cuda.so   sm_100a kernels + C ABI (include/psm.h)
+    poststackmig3d_b200/lib/libpsm_host.so   C++ host surface (include/psm_host.h)
+    poststackmig3d_b200/bin/poststackmig     the config.txt-driven migration binary
+nvcc cross-compiles for sm_100a without a GPU.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "lib")
+BIN = os.path.join(PKG, "bin")
+INC = os.path.join(ROOT, "include")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CXX = "/usr/bin/g++"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CUDA_SRC = [os.path.join(CSRC, "psm_cuda.cu")]
+CUDA_DEPS = CUDA_SRC + [os.path.join(CSRC, "psm_kernels.cuh"), os.path.join(INC, "psm.h")]
+HOST_SRC = [os.path.join(CSRC, "host", f) for f in
+            ("config.cpp", "segy.cpp", "velocity.cpp", "driver.cpp", "host_abi.cpp")]
+HOST_DEPS = HOST_SRC + [os.path.join(CSRC, "host", "host.hpp"),
+                        os.path.join(INC, "psm_host.h"), os.path.join(INC, "psm.h")]
+MAIN_SRC = os.path.join(CSRC, "host", "main.cpp")
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_cuda(force: bool = False, extra=()) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    out = os.path.join(LIB, "libpsm_cuda.so")
+    if force or extra or _stale(out, CUDA_DEPS):
+        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-shared", f"-I{INC}", *extra, "-o", out, *CUDA_SRC])
+    return out
+
+
+def build_host(force: bool = False) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    os.makedirs(BIN, exist_ok=True)
+    out = os.path.join(LIB, "libpsm_host.so")
+    if all(os.path.exists(s) for s in HOST_SRC):
+        if force or _stale(out, HOST_DEPS + [os.path.join(LIB, "libpsm_cuda.so")]):
+            _run([CXX, "-std=c++17", "-O2", "-fPIC", "-shared", "-fopenmp", f"-I{INC}",
+                  "-o", out, *HOST_SRC, f"-L{LIB}", "-lpsm_cuda", "-Wl,-rpath,$ORIGIN"])
+        exe = os.path.join(BIN, "poststackmig")
+        if force or _stale(exe, [MAIN_SRC, out]):
+            _run([CXX, "-std=c++17", "-O2", f"-I{INC}", "-o", exe, MAIN_SRC, f"-L{LIB}",
+                  "-lpsm_host", "-lpsm_cuda", "-Wl,-rpath,$ORIGIN/../lib"])
+    return out
+
+
+def build(force: bool = False) -> None:
+    build_cuda(force)
+    build_host(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

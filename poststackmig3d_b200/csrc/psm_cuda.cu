@@ -1,0 +1,515 @@
+// libpsm_cuda.so: C ABI (include/psm.h) over the sm_100a migration kernels (psm_kernels.cuh).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "psm.h"
+#include "psm_kernels.cuh"
+
+namespace {
+
+using psm::FwdParams;
+using psm::Job;
+
+constexpr size_t kFwdSmem =
+    ((sizeof(uint64_t) * 2 * psm::kStages + sizeof(psm::StageMeta) * psm::kStages +
+      sizeof(psm::TileStats) * psm::kTX + 127) &
+     ~size_t(127)) +
+    sizeof(float) * psm::kStages * psm::kStageCap;
+
+// Trace stride in HBM: n_t rounded up to 8 samples (32 B) so every trace starts 16 B aligned
+// for the TMA bulk copies; the tail samples stay zero.
+inline int trace_stride(int n_t) { return (n_t + 7) & ~7; }
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, n ? n : 16);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct Status {
+    int code = PSM_OK;
+    std::string msg;
+    int fail(int c, const std::string& m) {
+        code = c;
+        msg = m;
+        return c;
+    }
+};
+
+#define PSM_CUDA_TRY(st, call)                                                          \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return (st).fail(e_ == cudaErrorMemoryAllocation ? PSM_ERR_NOMEM : PSM_ERR_CUDA, \
+                             std::string(#call) + ": " + cudaGetErrorString(e_));        \
+    } while (0)
+
+// Launch the forward kernel for n_jobs jobs (template dispatch on J and amplitude mode).
+template <int J>
+cudaError_t launch_fwd_j(const FwdParams& P, int n_jobs, bool amp, cudaStream_t s) {
+    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + 32 * J - 1) / (32 * J), n_jobs);
+    dim3 block(32 * (psm::kTX + 1));
+    cudaError_t e;
+    if (amp) {
+        e = cudaFuncSetAttribute(psm::fwd_kernel<J, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
+        if (e != cudaSuccess) return e;
+        psm::fwd_kernel<J, true><<<grid, block, kFwdSmem, s>>>(P);
+    } else {
+        e = cudaFuncSetAttribute(psm::fwd_kernel<J, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
+        if (e != cudaSuccess) return e;
+        psm::fwd_kernel<J, false><<<grid, block, kFwdSmem, s>>>(P);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, cudaStream_t s) {
+    if (n_jobs <= 0 || P.n_ox <= 0 || P.n_t <= 0) return cudaSuccess;
+    if (P.n_t <= 64) return launch_fwd_j<2>(P, n_jobs, amp, s);
+    if (P.n_t <= 128) return launch_fwd_j<4>(P, n_jobs, amp, s);
+    return launch_fwd_j<8>(P, n_jobs, amp, s);
+}
+
+void fill_consts(FwdParams& P, float dt, float d_il, float d_xl, float tan2) {
+    P.inv_dt = 1.0f / dt;  // migration_kernel.cpp:44
+    P.idt2 = P.inv_dt * P.inv_dt;
+    P.d_il = d_il;
+    P.d_xl = d_xl;
+    P.inv_dxl = 1.0f / d_xl;
+    P.tan2 = tan2;
+    P.tanth = std::sqrt(std::max(tan2, 0.0f));
+    P.ntm1f = static_cast<float>(P.n_t) - 1.0f;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------- context
+
+struct psm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Status st;
+    bool have_geom = false, have_traces = false, have_vrms = false;
+    psm_geom g{};
+    int ns = 0;
+    std::vector<Job> jobs;       // one per distinct migrated inline
+    std::vector<Job> jobs_all;   // one per output row (term counting)
+    std::vector<std::pair<int, int>> copies;  // (dst row, src row) duplicated output rows
+    DevBuf data, vrms, image, d_jobs, d_jobs_all, il_pos, t0, err, count;
+};
+
+namespace {
+
+FwdParams volume_params(psm_ctx* c) {
+    FwdParams P{};
+    P.data = c->data.as<float>();
+    P.vrms = c->vrms.as<float>();
+    P.image = c->image.as<float>();
+    P.jobs = c->d_jobs.as<Job>();
+    P.il_pos = c->il_pos.as<int>();
+    P.t0 = c->t0.as<float>();
+    P.err = c->err.as<int>();
+    P.n_ci = c->g.n_il;
+    P.n_cx = c->g.n_xl;
+    P.n_t = c->g.n_t;
+    P.ns = c->ns;
+    P.n_vx = c->g.n_xl;
+    P.n_ox = c->g.n_ox;
+    P.xoff = -c->g.pad_xl;
+    fill_consts(P, c->g.dt, c->g.d_il, c->g.d_xl, c->g.tan2_theta);
+    return P;
+}
+
+int read_device_error(psm_ctx* c) {
+    int h = 0;
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(&h, c->err.p, sizeof(int), cudaMemcpyDeviceToHost,
+                                        c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    if (h) return c->st.fail(PSM_ERR_DEVICE, "kernel reported device error flags " +
+                                                 std::to_string(h));
+    return PSM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* psm_version(void) { return "poststackmig3d-b200 0.1 (sm_100a)"; }
+
+int psm_device_count(int* count) {
+    if (!count) return PSM_ERR_ARG;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    *count = n;
+    return PSM_OK;
+}
+
+int psm_create(psm_ctx** out, int device) {
+    if (!out) return PSM_ERR_ARG;
+    *out = nullptr;
+    psm_ctx* c = new (std::nothrow) psm_ctx();
+    if (!c) return PSM_ERR_NOMEM;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return PSM_ERR_CUDA;
+    }
+    *out = c;
+    return PSM_OK;
+}
+
+int psm_destroy(psm_ctx* c) {
+    if (!c) return PSM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->data.release();
+    c->vrms.release();
+    c->image.release();
+    c->d_jobs.release();
+    c->d_jobs_all.release();
+    c->il_pos.release();
+    c->t0.release();
+    c->err.release();
+    c->count.release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return PSM_OK;
+}
+
+const char* psm_last_error(const psm_ctx* c) { return c ? c->st.msg.c_str() : "null context"; }
+
+int psm_stream(psm_ctx* c, void** s) {
+    if (!c || !s) return PSM_ERR_ARG;
+    *s = c->stream;
+    return PSM_OK;
+}
+
+int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
+    if (!c || !g) return PSM_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (g->n_il <= 0 || g->n_xl <= 0 || g->n_t <= 0 || g->n_oi <= 0 || g->n_ox <= 0 ||
+        g->pad_il < 0 || g->pad_xl < 0 || g->m_il < 0 || !(g->dt > 0.0f) ||
+        !(g->d_il > 0.0f) || !(g->d_xl > 0.0f) || !(g->tan2_theta >= 0.0f))
+        return c->st.fail(PSM_ERR_ARG, "invalid geometry");
+    if (g->precision != PSM_F32)
+        return c->st.fail(PSM_ERR_UNSUPPORTED, "only PSM_F32 storage is built");
+    const int ns = trace_stride(g->n_t);
+    if (ns > psm::kStageCap)
+        return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t too large for the staging ring");
+    std::vector<int> center(g->n_oi);
+    for (int o = 0; o < g->n_oi; ++o) {
+        int cc = out_center ? out_center[o] : std::min(std::max(o - g->pad_il, 0), g->n_il - 1);
+        if (cc < 0 || cc >= g->n_il) return c->st.fail(PSM_ERR_ARG, "out_center out of range");
+        center[o] = cc;
+    }
+    c->g = *g;
+    c->ns = ns;
+    c->jobs.clear();
+    c->jobs_all.clear();
+    c->copies.clear();
+    std::vector<int> first_row(g->n_il, -1);
+    for (int o = 0; o < g->n_oi; ++o) {
+        const int cc = center[o];
+        // buffer inlines (migration_kernel.cpp:404-409)
+        const int rs = std::max(0, cc - g->m_il), re = std::min(g->n_il, cc + g->m_il + 1);
+        Job j;
+        j.row = o;
+        j.vrow = cc;
+        j.pos = cc;
+        j.i0 = std::max(0, rs - g->pad_il);
+        j.i1 = std::min(g->n_il, re + g->pad_il);
+        c->jobs_all.push_back(j);
+        if (first_row[cc] < 0) {
+            first_row[cc] = o;
+            c->jobs.push_back(j);
+        } else {
+            c->copies.emplace_back(o, first_row[cc]);
+        }
+    }
+    const size_t n_tr = static_cast<size_t>(g->n_il) * g->n_xl;
+    PSM_CUDA_TRY(c->st, c->data.ensure(n_tr * ns * sizeof(float)));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->data.p, 0, n_tr * ns * sizeof(float), c->stream));
+    PSM_CUDA_TRY(c->st, c->vrms.ensure(n_tr * g->n_t * sizeof(float)));
+    PSM_CUDA_TRY(c->st, c->image.ensure(static_cast<size_t>(g->n_oi) * g->n_ox * g->n_t *
+                                        sizeof(float)));
+    PSM_CUDA_TRY(c->st, c->d_jobs.ensure(c->jobs.size() * sizeof(Job)));
+    PSM_CUDA_TRY(c->st, c->d_jobs_all.ensure(c->jobs_all.size() * sizeof(Job)));
+    PSM_CUDA_TRY(c->st, c->il_pos.ensure(g->n_il * sizeof(int)));
+    PSM_CUDA_TRY(c->st, c->t0.ensure(g->n_t * sizeof(float)));
+    PSM_CUDA_TRY(c->st, c->err.ensure(sizeof(int)));
+        std::vector<int> pos(g->n_il);
+    for (int i = 0; i < g->n_il; ++i) pos[i] = i;
+    std::vector<float> t0(g->n_t);
+    for (int i = 0; i < g->n_t; ++i)
+        t0[i] = static_cast<float>(static_cast<double>(i) * g->dt_seconds);  // main.cpp:216
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_jobs.p, c->jobs.data(), c->jobs.size() * sizeof(Job),
+                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_jobs_all.p, c->jobs_all.data(),
+                                        c->jobs_all.size() * sizeof(Job),
+                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->il_pos.p, pos.data(), pos.size() * sizeof(int),
+                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->t0.p, t0.data(), t0.size() * sizeof(float),
+                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    c->have_geom = true;
+    c->have_traces = c->have_vrms = false;
+    return PSM_OK;
+}
+
+int psm_set_traces(psm_ctx* c, const float* data) {
+    if (!c || !data) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.p, c->ns * sizeof(float), data,
+                                          c->g.n_t * sizeof(float), c->g.n_t * sizeof(float),
+                                          n_tr, cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    c->have_traces = true;
+    return PSM_OK;
+}
+
+int psm_set_vrms(psm_ctx* c, const float* vrms) {
+    if (!c || !vrms) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    const size_t n = static_cast<size_t>(c->g.n_il) * c->g.n_xl * c->g.n_t;
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.p, vrms, n * sizeof(float),
+                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    c->have_vrms = true;
+    return PSM_OK;
+}
+
+int psm_forward_async(psm_ctx* c) {
+    if (!c) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_traces || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry, traces and vrms must be set");
+    cudaSetDevice(c->device);
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    FwdParams P = volume_params(c);
+    PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
+                                   c->g.amp_correction != 0, c->stream));
+    // padded output inlines repeat the migrated edge inline (main.cpp:268-285)
+    const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
+    for (const auto& cp : c->copies)
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.as<float>() + cp.first * row,
+                                            c->image.as<float>() + cp.second * row,
+                                            row * sizeof(float), cudaMemcpyDeviceToDevice,
+                                            c->stream));
+    return PSM_OK;
+}
+
+int psm_synchronize(psm_ctx* c) {
+    if (!c) return PSM_ERR_ARG;
+    cudaSetDevice(c->device);
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int psm_image_device(psm_ctx* c, float** dev_image) {
+    if (!c || !dev_image) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    *dev_image = c->image.as<float>();
+    return PSM_OK;
+}
+
+int psm_get_image(psm_ctx* c, float* image) {
+    if (!c || !image) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    const size_t n = static_cast<size_t>(c->g.n_oi) * c->g.n_ox * c->g.n_t;
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image, c->image.p, n * sizeof(float),
+                                        cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int psm_forward(psm_ctx* c, float* image) {
+    if (!c || !image) return PSM_ERR_ARG;
+    int r = psm_forward_async(c);
+    if (r) return r;
+    return psm_get_image(c, image);
+}
+
+int psm_count_terms_rows(psm_ctx* c, int64_t* per_row) {
+    if (!c || !per_row) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry and vrms must be set");
+    cudaSetDevice(c->device);
+    FwdParams P = volume_params(c);
+    P.jobs = c->d_jobs_all.as<Job>();
+    const size_t nj = c->jobs_all.size();
+    PSM_CUDA_TRY(c->st, c->count.ensure(nj * sizeof(unsigned long long)));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->count.p, 0, nj * sizeof(unsigned long long),
+                                        c->stream));
+    psm::count_kernel<<<dim3(c->g.n_ox, static_cast<unsigned>(nj)), 256, 0, c->stream>>>(
+        P, c->count.as<unsigned long long>());
+    PSM_CUDA_TRY(c->st, cudaGetLastError());
+    std::vector<unsigned long long> h(nj);
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(h.data(), c->count.p, nj * sizeof(unsigned long long),
+                                        cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    for (size_t j = 0; j < nj; ++j) per_row[c->jobs_all[j].row] = static_cast<int64_t>(h[j]);
+    return PSM_OK;
+}
+
+int psm_count_terms(psm_ctx* c, int64_t* n_terms) {
+    if (!c || !n_terms) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    std::vector<int64_t> rows(c->g.n_oi, 0);
+    int r = psm_count_terms_rows(c, rows.data());
+    if (r) return r;
+    int64_t s = 0;
+    for (int64_t v : rows) s += v;
+    *n_terms = s;
+    return PSM_OK;
+}
+
+// ---------------------------------------------------------------------------- per inline
+
+namespace {
+struct InlineStaging {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    Status st;
+    DevBuf data, vel, out, job, il_pos, t0, err;
+    ~InlineStaging() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+thread_local std::unique_ptr<InlineStaging> tl_staging;
+thread_local std::string tl_inline_error;
+}  // namespace
+
+int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_buf_xl,
+                         size_t n_t, const float* velocity_slice, float* output_slice,
+                         size_t n_out_xl, const int32_t* il_pos_indices,
+                         const int32_t* /*xl_pos_indices*/, int32_t current_il_pos,
+                         int32_t current_xl_start, float dt, const float* t0_times,
+                         float tan_theta_sq, float inline_bin_size,
+                         float crossline_bin_size, int amp_correction) {
+    tl_inline_error.clear();
+    if (n_out_xl == 0 || n_t == 0) return PSM_OK;  // migration_kernel.cpp:35-37
+    if (!output_slice || !t0_times || (n_buf_il && (!input_buffer || !il_pos_indices)) ||
+        (n_buf_xl && !velocity_slice)) {
+        tl_inline_error = "null pointer argument";
+        return PSM_ERR_ARG;
+    }
+    if (n_buf_il > 0x7fffffff || n_buf_xl > 0x7fffffff || n_t > 0x7fffffff ||
+        n_out_xl > 0x7fffffff) {
+        tl_inline_error = "size too large";
+        return PSM_ERR_ARG;
+    }
+    const int ns = trace_stride(static_cast<int>(n_t));
+    if (ns > psm::kStageCap) {
+        tl_inline_error = "n_t too large for the staging ring";
+        return PSM_ERR_UNSUPPORTED;
+    }
+    if (!tl_staging) tl_staging.reset(new (std::nothrow) InlineStaging());
+    InlineStaging* S = tl_staging.get();
+    if (!S) return PSM_ERR_NOMEM;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    auto fail = [&](int code, const std::string& m) {
+        tl_inline_error = m;
+        return code;
+    };
+#define PSM_INL_TRY(call)                                                                   \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? PSM_ERR_NOMEM : PSM_ERR_CUDA,     \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    } while (0)
+    if (S->device != dev || !S->stream) {
+        if (S->stream) cudaStreamDestroy(S->stream);
+        S->stream = nullptr;
+        PSM_INL_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+        S->device = dev;
+    }
+    const size_t n_tr = n_buf_il * n_buf_xl;
+    PSM_INL_TRY(S->data.ensure(std::max<size_t>(n_tr, 1) * ns * sizeof(float)));
+    PSM_INL_TRY(S->vel.ensure(std::max<size_t>(n_buf_xl, 1) * n_t * sizeof(float)));
+    PSM_INL_TRY(S->out.ensure(n_out_xl * n_t * sizeof(float)));
+    PSM_INL_TRY(S->job.ensure(sizeof(Job)));
+    PSM_INL_TRY(S->il_pos.ensure(std::max<size_t>(n_buf_il, 1) * sizeof(int)));
+    PSM_INL_TRY(S->t0.ensure(n_t * sizeof(float)));
+    PSM_INL_TRY(S->err.ensure(sizeof(int)));
+    cudaStream_t s = S->stream;
+    if (n_tr) {
+        PSM_INL_TRY(cudaMemsetAsync(S->data.p, 0, n_tr * ns * sizeof(float), s));
+        PSM_INL_TRY(cudaMemcpy2DAsync(S->data.p, ns * sizeof(float), input_buffer,
+                                      n_t * sizeof(float), n_t * sizeof(float), n_tr,
+                                      cudaMemcpyHostToDevice, s));
+    }
+    if (n_buf_xl)
+        PSM_INL_TRY(cudaMemcpyAsync(S->vel.p, velocity_slice, n_buf_xl * n_t * sizeof(float),
+                                    cudaMemcpyHostToDevice, s));
+    if (n_buf_il)
+        PSM_INL_TRY(cudaMemcpyAsync(S->il_pos.p, il_pos_indices, n_buf_il * sizeof(int),
+                                    cudaMemcpyHostToDevice, s));
+    PSM_INL_TRY(cudaMemcpyAsync(S->t0.p, t0_times, n_t * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    // migration_kernel.cpp:48-49
+    const int32_t cur = (current_il_pos >= 0 && current_il_pos < static_cast<int32_t>(n_buf_il))
+                            ? il_pos_indices[current_il_pos]
+                            : 0;
+    Job j{0, 0, cur, 0, static_cast<int>(n_buf_il)};
+    PSM_INL_TRY(cudaMemcpyAsync(S->job.p, &j, sizeof(Job), cudaMemcpyHostToDevice, s));
+    PSM_INL_TRY(cudaMemsetAsync(S->err.p, 0, sizeof(int), s));
+    FwdParams P{};
+    P.data = S->data.as<float>();
+    P.vrms = S->vel.as<float>();
+    P.image = S->out.as<float>();
+    P.jobs = S->job.as<Job>();
+    P.il_pos = S->il_pos.as<int>();
+    P.t0 = S->t0.as<float>();
+    P.err = S->err.as<int>();
+    P.n_ci = static_cast<int>(n_buf_il);
+    P.n_cx = static_cast<int>(n_buf_xl);
+    P.n_t = static_cast<int>(n_t);
+    P.ns = ns;
+    P.n_vx = static_cast<int>(n_buf_xl);
+    P.n_ox = static_cast<int>(n_out_xl);
+    P.xoff = current_xl_start;
+    fill_consts(P, dt, inline_bin_size, crossline_bin_size, tan_theta_sq);
+    PSM_INL_TRY(launch_fwd(P, 1, amp_correction != 0, s));
+    PSM_INL_TRY(cudaMemcpyAsync(output_slice, S->out.p, n_out_xl * n_t * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+    int h = 0;
+    PSM_INL_TRY(cudaMemcpyAsync(&h, S->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PSM_INL_TRY(cudaStreamSynchronize(s));
+    if (h) return fail(PSM_ERR_DEVICE, "kernel reported device error flags " + std::to_string(h));
+#undef PSM_INL_TRY
+    return PSM_OK;
+}
+
+const char* psm_kirchhoff_inline_error(void) { return tl_inline_error.c_str(); }
+
+}  // extern "C"

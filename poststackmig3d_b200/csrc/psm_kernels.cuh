@@ -1,0 +1,524 @@
+// Device code of the B200 Kirchhoff post-stack 3D time migration (sm_100a).
+//
+// The operator is the reference's diffraction summation (sergeevsn/poststackmig3d,
+// src/migration_kernel.cpp:17-383): for every output sample (inline c, crossline x, time t0)
+//     out = sum over input traces (i, k) with r^2 = dx^2 + dy^2 <= (v t0 / 2)^2 tan^2(theta)
+//           and floor(t / dt) < n_t - 1 of  interp(trace(i,k), t / dt) / (t v^2)
+// with t = sqrt(t0^2 + 4 r^2 / v^2), v the output point's Vrms, interp the linear rule
+// fma(frac, d[lo+1] - d[lo], d[lo]) (simdInterpolate, :544-550).
+//
+// Work decomposition (one CTA):
+//   * one output row ("job": an output inline), TX consecutive output crosslines, TT
+//     consecutive output samples (a "tile");
+//   * warp 0 is the producer: it enumerates the input traces that can reach the tile, derives
+//     for each a time window [ws, we) that covers every unmasked term of the tile, and stages
+//     the windows into shared memory with TMA bulk copies (cp.async.bulk) into a ring of
+//     kStages buffers guarded by mbarriers;
+//   * warps 1..TX are consumers: warp w owns output crossline x0 + w-1 and holds, per lane,
+//     J samples t0 = T0 + lane + 32 j.  For each staged trace the per-trace quantities
+//     (dy, r^2, window base) are warp-uniform; each lane evaluates its J terms from shared
+//     memory.
+// Every wait is bounded: on expiry the kernel records PSM_DEV_ERR_TIMEOUT in *err and leaves.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace psm {
+
+constexpr int kTX = 8;            // output crosslines per CTA (one consumer warp each)
+constexpr int kStages = 2;        // TMA ring depth
+constexpr int kStageCap = 12288;  // floats per ring stage (48 KB)
+constexpr int kMaxG = 32;         // traces per ring stage
+constexpr unsigned kWaitLimit = 1u << 26;  // bounded mbarrier polls
+
+constexpr int PSM_DEV_ERR_TIMEOUT = 1;
+constexpr int PSM_DEV_ERR_WINDOW = 2;  // debug-bounds build only
+
+// One output inline of a launch.
+struct Job {
+    int row;   // output image row
+    int vrow;  // Vrms plane (cube inline of the output point's velocity)
+    int pos;   // inline position of the output point (dx = (il_pos[i] - pos) * d_il)
+    int i0;    // cube inlines [i0, i1) form the buffer (migration_kernel.cpp:404-409)
+    int i1;
+};
+
+struct FwdParams {
+    const float* data;    // [n_ci][n_cx][ns]  traces, ns-sample stride, 16 B aligned
+    const float* vrms;    // [n_vrow][n_vx][n_t] Vrms of output points
+    float* image;         // [rows][n_ox][n_t]
+    const Job* jobs;
+    const int* il_pos;    // [n_ci] inline positions
+    const float* t0;      // [n_t]
+    int* err;
+    int n_ci, n_cx, n_t, ns;
+    int n_vx;             // crosslines of a Vrms plane
+    int n_ox;             // output crosslines per row
+    int xoff;             // cube / Vrms crossline of output x is x + xoff
+    float inv_dt, idt2, d_il, d_xl, inv_dxl, tan2, tanth, ntm1f;
+};
+
+struct StageMeta {
+    int count;  // traces in this stage, -1 = end of stream
+    float dx2;  // (dx)^2 of the stage's input inline
+    int k[kMaxG];    // cube crossline of each trace
+    int off[kMaxG];  // float offset of the trace window in the stage buffer
+    int ws[kMaxG];   // first sample of the window
+    int lim[kMaxG];  // window length - 2 (largest valid lo - ws)
+};
+
+struct TileStats {
+    float vmin, vmax, md2max, t0min, t0max;
+    int any;
+};
+
+// ----------------------------------------------------------------------------- PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.release.cta.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+            smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false (and *err set) when the limit expires.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+    for (unsigned it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(err, PSM_DEV_ERR_TIMEOUT);
+    return false;
+}
+
+// TMA bulk copy global -> shared, completion counted on an mbarrier (bytes % 16 == 0,
+// both addresses 16 B aligned).
+__device__ __forceinline__ void tma_load_1d(void* dst_smem, const void* src, uint32_t bytes,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst_smem)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ----------------------------------------------------------------------------- point setup
+
+// Per output sample constants in the reference's FP32 order (migration_kernel.cpp:115-144).
+// Division and products are pinned to round-to-nearest so the masks see the same numbers
+// as the reference build.
+struct PointConst {
+    bool valid;
+    float t0sq, f4, md2, vsq;
+};
+
+__device__ __forceinline__ PointConst point_const(float v, float t0v, float tan2) {
+    PointConst p;
+    p.valid = (v >= 1e-5f) && (t0v >= 1e-5f);                 // :121
+    p.t0sq = __fmul_rn(t0v, t0v);                              // :125
+    p.vsq = __fmul_rn(v, v);                                   // :127
+    float inv_vsq = __fdiv_rn(1.0f, __fadd_rn(p.vsq, 1e-10f)); // :128
+    p.f4 = __fmul_rn(4.0f, inv_vsq);                           // :129
+    float vth = __fmul_rn(__fmul_rn(v, t0v), 0.5f);            // :133
+    p.md2 = __fmul_rn(__fmul_rn(vth, vth), tan2);              // :134
+    return p;
+}
+
+// dx^2 of a buffer inline (migration_kernel.cpp:51-56).
+__device__ __forceinline__ float inline_dx2(int ipos, int pos, float d_il) {
+    float dx = __fmul_rn(static_cast<float>(ipos - pos), d_il);
+    return __fmul_rn(dx, dx);
+}
+
+// r^2 of a trace at crossline distance dk (migration_kernel.cpp:197-204 / :282-284, with the
+// multiply-add fused as the reference's GCC build fuses it).
+__device__ __forceinline__ float trace_r2(int dk, float d_xl, float dx2) {
+    float dy = __fmul_rn(static_cast<float>(dk), d_xl);
+    return __fmaf_rn(dy, dy, dx2);
+}
+
+// ----------------------------------------------------------------------------- forward
+
+// Producer: derive the window of trace (i, kc) for the tile; size 0 = no terms.
+__device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats& S, int xa,
+                                             int xb, float dx2, int kc, int* ws_out,
+                                             int* size_out) {
+    *ws_out = 0;
+    *size_out = 0;
+    int dkmin = kc < xa ? xa - kc : (kc > xb ? kc - xb : 0);
+    int dkmax = max(abs(kc - xa), abs(kc - xb));
+    float dymin = static_cast<float>(dkmin) * P.d_xl;
+    float dymax = static_cast<float>(dkmax) * P.d_xl;
+    float rmin2 = fmaf(dymin, dymin, dx2);
+    float rmax2 = fmaf(dymax, dymax, dx2);
+    if (rmin2 > S.md2max * 1.0001f + 1e-6f) return;
+    // Unmasked terms need r <= v t0 tan / 2, so t0 >= 2 r_min / (v_max tan).
+    float t0lo = S.t0min;
+    if (P.tanth > 0.0f) t0lo = fmaxf(t0lo, 2.0f * sqrtf(rmin2) / (S.vmax * P.tanth));
+    float tlo = sqrtf(fmaf(t0lo, t0lo, 4.0f * rmin2 / fmaf(S.vmax, S.vmax, 1e-10f)));
+    // and t^2 = t0^2 + f4 r^2 <= t0^2 (1 + tan^2) inside the aperture.
+    float thi2 = fminf(fmaf(S.t0max, S.t0max, 4.0f * rmax2 / fmaf(S.vmin, S.vmin, 1e-10f)),
+                       S.t0max * S.t0max * (1.0f + P.tan2) * 1.0001f);
+    float slo = tlo * P.inv_dt;
+    float shi = fminf(sqrtf(thi2) * P.inv_dt, 1.0e9f);
+    int lolo = max(static_cast<int>(floorf(slo)) - 2, 0);
+    int lohi = min(static_cast<int>(floorf(shi)) + 2, P.n_t - 2);
+    if (lolo > lohi) return;
+    int ws = lolo & ~3;
+    int we = (lohi + 2 + 3) & ~3;  // samples up to lohi + 1, rounded to 16 B
+    *ws_out = ws;
+    *size_out = we - ws;
+}
+
+template <int J, bool AMP>
+__global__ void __launch_bounds__(32 * (kTX + 1))
+    fwd_kernel(const FwdParams P) {
+    constexpr int TT = 32 * J;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
+    uint64_t* empty = full + kStages;
+    StageMeta* meta = reinterpret_cast<StageMeta*>(empty + kStages);
+    TileStats* wstats = reinterpret_cast<TileStats*>(meta + kStages);
+    float* sbuf = reinterpret_cast<float*>(
+        smem_raw + ((sizeof(uint64_t) * 2 * kStages + sizeof(StageMeta) * kStages +
+                     sizeof(TileStats) * kTX + 127) &
+                    ~size_t(127)));
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const Job job = P.jobs[blockIdx.z];
+    const int x0 = blockIdx.x * kTX;
+    const int T0 = blockIdx.y * TT;
+
+    // ---- consumers: per-sample constants and tile statistics
+    float t02s[J], f4s[J], md2s[J], acc[J], blkmax[J];
+    float warpmax = -1.0f;
+    const int x = x0 + warp - 1;
+    const int xv = x + P.xoff;
+    if (warp > 0) {
+        const bool xvalid = x < P.n_ox && xv >= 0 && xv < P.n_vx;
+        const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
+                                    (xvalid ? xv : 0)) * P.n_t;
+        float vmin = 3.0e38f, vmax = 0.0f, md2max = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const int t = T0 + 32 * j + lane;
+            float v = 0.0f, t0v = 0.0f;
+            if (xvalid && t < P.n_t) {
+                v = __ldg(vp + t);
+                t0v = __ldg(P.t0 + t);
+            }
+            PointConst pc = point_const(v, t0v, P.tan2);
+            acc[j] = 0.0f;
+            if (pc.valid) {
+                t02s[j] = pc.t0sq * P.idt2;
+                f4s[j] = pc.f4 * P.idt2;
+                md2s[j] = pc.md2;
+                vmin = fminf(vmin, v);
+                vmax = fmaxf(vmax, v);
+                md2max = fmaxf(md2max, pc.md2);
+                t0min = fminf(t0min, t0v);
+                t0max = fmaxf(t0max, t0v);
+            } else {
+                t02s[j] = 1.0f;
+                f4s[j] = 0.0f;
+                md2s[j] = -1.0f;
+            }
+            blkmax[j] = warp_max(md2s[j]);
+            warpmax = fmaxf(warpmax, blkmax[j]);
+        }
+        vmin = warp_min(vmin);
+        vmax = warp_max(vmax);
+        md2max = warp_max(md2max);
+        t0min = warp_min(t0min);
+        t0max = warp_max(t0max);
+        if (lane == 0) {
+            TileStats s;
+            s.vmin = vmin;
+            s.vmax = vmax;
+            s.md2max = md2max;
+            s.t0min = t0min;
+            s.t0max = t0max;
+            s.any = md2max >= 0.0f;
+            wstats[warp - 1] = s;
+        }
+    } else if (lane == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kTX);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    if (warp == 0) {
+        // ---------------------------------------------------------------- producer
+        TileStats S;
+        S.vmin = 3.0e38f;
+        S.vmax = 0.0f;
+        S.md2max = -1.0f;
+        S.t0min = 3.0e38f;
+        S.t0max = 0.0f;
+        S.any = 0;
+        for (int w = 0; w < kTX; ++w) {
+            TileStats s = wstats[w];
+            if (!s.any) continue;
+            S.any = 1;
+            S.vmin = fminf(S.vmin, s.vmin);
+            S.vmax = fmaxf(S.vmax, s.vmax);
+            S.md2max = fmaxf(S.md2max, s.md2max);
+            S.t0min = fminf(S.t0min, s.t0min);
+            S.t0max = fmaxf(S.t0max, s.t0max);
+        }
+        // cube crossline range of the tile's output points
+        const int xa = max(x0 + P.xoff, 0);
+        const int xb = min(min(x0 + kTX, P.n_ox) - 1 + P.xoff, P.n_vx - 1);
+        uint32_t it = 0;
+        bool alive = true;
+        if (S.any && xa <= xb) {
+            for (int i = job.i0; i < job.i1 && alive; ++i) {
+                const float dx2 = inline_dx2(__ldg(P.il_pos + i), job.pos, P.d_il);
+                if (dx2 > S.md2max) continue;
+                const int K = static_cast<int>(sqrtf(fmaxf(S.md2max - dx2, 0.0f)) * P.inv_dxl) + 2;
+                const int klo = max(0, xa - K);
+                const int khi = min(P.n_cx - 1, xb + K);
+                const float* plane = P.data + static_cast<size_t>(i) * P.n_cx * P.ns;
+                int k = klo;
+                while (k <= khi) {
+                    const int kk = k + lane;
+                    int ws = 0, size = 0;
+                    if (kk <= khi) trace_window(P, S, xa, xb, dx2, kk, &ws, &size);
+                    // inclusive prefix sum of window sizes
+                    int cum = size;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        int n = __shfl_up_sync(0xffffffffu, cum, o);
+                        if (lane >= o) cum += n;
+                    }
+                    const bool take = cum <= kStageCap;
+                    const unsigned takemask = __ballot_sync(0xffffffffu, take);
+                    const int consumed = __popc(takemask);
+                    const unsigned nzmask = __ballot_sync(0xffffffffu, take && size > 0);
+                    const int n = __popc(nzmask);
+                    if (n > 0) {
+                        const int stage = it % kStages;
+                        const uint32_t par = ((it / kStages) & 1u) ^ 1u;
+                        int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
+                        if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                            alive = false;
+                            break;
+                        }
+                        StageMeta& m = meta[stage];
+                        const int total = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
+                        if (take && size > 0) {
+                            const int slot = __popc(nzmask & ((1u << lane) - 1u));
+                            m.k[slot] = kk;
+                            m.off[slot] = cum - size;
+                            m.ws[slot] = ws;
+                            m.lim[slot] = size - 2;
+                        }
+                        if (lane == 0) {
+                            m.count = n;
+                            m.dx2 = dx2;
+                        }
+                        __threadfence_block();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive_expect_tx(&full[stage], total * 4u);
+                        __syncwarp();
+                        if (take && size > 0)
+                            tma_load_1d(sbuf + stage * kStageCap + (cum - size),
+                                        plane + static_cast<size_t>(kk) * P.ns + ws,
+                                        static_cast<uint32_t>(size) * 4u, &full[stage]);
+                        ++it;
+                    }
+                    k += consumed;
+                }
+            }
+        }
+        // end-of-stream marker
+        if (alive && lane == 0) {
+            const int stage = it % kStages;
+            const uint32_t par = ((it / kStages) & 1u) ^ 1u;
+            if (mbar_wait(&empty[stage], par, P.err)) {
+                meta[stage].count = -1;
+                __threadfence_block();
+                mbar_arrive(&full[stage]);
+            }
+        }
+        return;
+    }
+
+    // -------------------------------------------------------------------- consumers
+    uint32_t it = 0;
+    while (true) {
+        const int stage = it % kStages;
+        const uint32_t par = (it / kStages) & 1u;
+        if (!mbar_wait(&full[stage], par, P.err)) break;
+        const StageMeta& m = meta[stage];
+        const int cnt = m.count;
+        if (cnt < 0) break;
+        const float dx2 = m.dx2;
+        const float* sb = sbuf + stage * kStageCap;
+        for (int g = 0; g < cnt; ++g) {
+            const int kc = m.k[g];
+            const float r2 = trace_r2(kc - xv, P.d_xl, dx2);
+            if (r2 > warpmax) continue;
+            const float* tb = sb + m.off[g];
+            const int ws = m.ws[g];
+            const unsigned lim = static_cast<unsigned>(m.lim[g]);
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                if (r2 > blkmax[j]) continue;
+                const float t2 = __fmaf_rn(f4s[j], r2, t02s[j]);  // (t / dt)^2
+                const float q = rsqrtf(t2);                        // dt / t
+                const float s = t2 * q;                            // t / dt
+                if (r2 <= md2s[j] && s < P.ntm1f) {
+                    const float mm = __fadd_rd(s, 8388608.0f);
+                    const int lo = __float_as_int(mm) - 0x4B000000;  // floor(s)
+                    const float fr = s - (mm - 8388608.0f);
+#ifdef PSM_DEBUG_BOUNDS
+                    if (static_cast<unsigned>(lo - ws) > lim) atomicOr(P.err, PSM_DEV_ERR_WINDOW);
+#endif
+                    const unsigned idx = min(static_cast<unsigned>(lo - ws), lim);
+                    const float a = tb[idx];
+                    const float b = tb[idx + 1];
+                    const float val = __fmaf_rn(fr, b - a, a);
+                    if (AMP)
+                        acc[j] = __fmaf_rn(val, q, acc[j]);
+                    else
+                        acc[j] += val;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stage]);
+        ++it;
+    }
+
+    // ---- write the tile: weight 1/(t v^2) = (dt/t) * inv_dt / v^2 applied per output sample
+    if (x < P.n_ox) {
+        const bool xvalid = xv >= 0 && xv < P.n_vx;
+        const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
+                                    (xvalid ? xv : 0)) * P.n_t;
+        float* op = P.image + (static_cast<size_t>(job.row) * P.n_ox + x) * P.n_t;
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const int t = T0 + 32 * j + lane;
+            if (t < P.n_t) {
+                float o = 0.0f;
+                if (md2s[j] >= 0.0f) {
+                    if (AMP) {
+                        const float v = __ldg(vp + t);
+                        o = acc[j] * __fdiv_rn(P.inv_dt, __fmul_rn(v, v));
+                    } else {
+                        o = acc[j];
+                    }
+                }
+                op[t] = o;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------- term count
+
+// Largest crossline distance d >= 0 whose term passes both masks for this output sample,
+// or -1.  Both masks are monotone in r^2, so the passing crosslines are |k - x| <= d.
+__device__ __forceinline__ bool term_pass(int d, float d_xl, float dx2, float md2, float f4s,
+                                          float t02s, float ntm1f) {
+    const float r2 = trace_r2(d, d_xl, dx2);
+    if (!(r2 <= md2)) return false;
+    const float t2 = __fmaf_rn(f4s, r2, t02s);
+    const float s = t2 * rsqrtf(t2);
+    return s < ntm1f;
+}
+
+// One block per (job, output crossline); threads stride over t.  out[job] += terms.
+__global__ void count_kernel(const FwdParams P, unsigned long long* out) {
+    __shared__ unsigned long long wsum[32];
+    const int x = blockIdx.x;
+    const Job job = P.jobs[blockIdx.y];
+    const int xv = x + P.xoff;
+    unsigned long long local = 0;
+    for (int t = threadIdx.x; t < P.n_t; t += blockDim.x) {
+        if (xv < 0 || xv >= P.n_vx) break;
+        const float v = P.vrms[(static_cast<size_t>(job.vrow) * P.n_vx + xv) * P.n_t + t];
+        const PointConst pc = point_const(v, P.t0[t], P.tan2);
+        if (!pc.valid) continue;
+        const float f4s = pc.f4 * P.idt2, t02s = pc.t0sq * P.idt2;
+        for (int i = job.i0; i < job.i1; ++i) {
+            const float dx2 = inline_dx2(P.il_pos[i], job.pos, P.d_il);
+            if (dx2 > pc.md2) continue;
+            if (!term_pass(0, P.d_xl, dx2, pc.md2, f4s, t02s, P.ntm1f)) continue;
+            int d = static_cast<int>(sqrtf(fmaxf(pc.md2 - dx2, 0.0f)) * P.inv_dxl);
+            // the range mask: t^2 < ntm1^2 -> r^2 < (ntm1^2 - t02s) / f4s
+            if (f4s > 0.0f) {
+                const float r2s = (P.ntm1f * P.ntm1f - t02s) / f4s - dx2;
+                if (r2s <= 0.0f)
+                    d = 0;
+                else
+                    d = min(d, static_cast<int>(sqrtf(r2s) * P.inv_dxl) + 1);
+            }
+            d = min(d, P.n_cx + 1);
+            while (d > 0 && !term_pass(d, P.d_xl, dx2, pc.md2, f4s, t02s, P.ntm1f)) --d;
+            while (d <= P.n_cx && term_pass(d + 1, P.d_xl, dx2, pc.md2, f4s, t02s, P.ntm1f)) ++d;
+            const int lo = max(0, xv - d), hi = min(P.n_cx - 1, xv + d);
+            if (hi >= lo) local += static_cast<unsigned long long>(hi - lo + 1);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += wsum[w];
+        if (s) atomicAdd(out + blockIdx.y, s);
+    }
+}
+
+}  // namespace psm

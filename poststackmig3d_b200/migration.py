@@ -1,0 +1,291 @@
+"""Python face of the migration operator (the reference's MigrationKernel seam).
+
+* MigrationKernel.kirchhoff_kernel_3d_with_padding mirrors
+  MigrationKernel::kirchhoffKernel3DWithPadding (include/migration_kernel.h:16-31) argument by
+  argument and runs it on the GPU through psm_kirchhoff_inline.
+* Migrator holds a whole cube resident in HBM (psm_ctx) and migrates every output inline in
+  one launch; plan_geometry() derives its parameters the way src/main.cpp:124-217 does for a
+  regular grid.
+Everything here calls libpsm_cuda.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import PsmGeom, check
+
+PRECISIONS = {"f32": 0, "bf16": 1, "f16": 2}
+
+
+def _addr(a) -> int:
+    """Host address of a C-contiguous float32 numpy array or CPU torch tensor."""
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda:
+            raise ValueError("host buffer expected")
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    raise TypeError(type(a))
+
+
+def _f32(a, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape != tuple(shape):
+        a = a.reshape(shape)
+    return a
+
+
+# ----------------------------------------------------------------------------- geometry
+
+
+def tan2_theta(angle_deg: float) -> float:
+    """src/main.cpp:188-189: float(tan(angle * pi / 180)) squared in float."""
+    t = np.float32(math.tan(angle_deg * math.pi / 180.0))
+    return float(np.float32(t * t))
+
+
+def max_aperture_il(max_v: float, n_t: int, dt_seconds: float, tan2: float,
+                    inline_step: float) -> int:
+    """src/main.cpp:197-201 (the float/double mix kept)."""
+    max_t = (n_t - 1) * dt_seconds
+    rad = np.float32(np.float32(np.float32(max_v) * np.float32(max_t)) / np.float32(2.0))
+    rad = np.float32(rad * np.sqrt(np.float32(tan2), dtype=np.float32))
+    return int(float(rad) / inline_step) + 1
+
+
+def padded_labels(labels: Sequence[int], pad: int) -> np.ndarray:
+    """src/main.cpp:144-172: extend by pad steps of labels[1]-labels[0] on both sides."""
+    labels = np.asarray(labels, dtype=np.int64)
+    if pad > 0 and len(labels) > 1:
+        step = int(labels[1] - labels[0])
+        return np.arange(labels[0] - pad * step, labels[-1] + pad * step + 1, step,
+                         dtype=np.int64)
+    return labels.copy()
+
+
+def output_centers(in_labels: Sequence[int], out_labels: Sequence[int]) -> np.ndarray:
+    """src/main.cpp:258-288: the real inline index each output inline migrates."""
+    in_labels = np.asarray(in_labels, dtype=np.int64)
+    res = np.empty(len(out_labels), dtype=np.int32)
+    n = len(in_labels)
+    for o, lab in enumerate(out_labels):
+        hit = np.nonzero(in_labels == lab)[0]
+        if len(hit):
+            res[o] = hit[0]
+        elif lab < in_labels[0]:
+            res[o] = 0
+        elif lab > in_labels[-1]:
+            res[o] = n - 1
+        else:
+            res[o] = int(np.argmin(np.abs(in_labels - lab)))  # first minimum, as :278-284
+    return res
+
+
+@dataclasses.dataclass
+class Geometry:
+    n_il: int
+    n_xl: int
+    n_t: int
+    dt_seconds: float
+    d_il: float
+    d_xl: float
+    tan2: float
+    m_il: int
+    pad_il: int
+    pad_xl: int
+    n_oi: int
+    n_ox: int
+    out_center: np.ndarray
+    amp: bool = True
+    precision: str = "f32"
+
+    @property
+    def dt(self) -> float:
+        return float(np.float32(self.dt_seconds))
+
+    def t0(self) -> np.ndarray:
+        """src/main.cpp:214-217."""
+        return np.array([np.float32(i * self.dt_seconds) for i in range(self.n_t)],
+                        dtype=np.float32)
+
+    def to_c(self) -> PsmGeom:
+        return PsmGeom(self.n_il, self.n_xl, self.n_t, self.pad_il, self.pad_xl, self.n_oi,
+                       self.n_ox, self.m_il, int(bool(self.amp)), PRECISIONS[self.precision],
+                       np.float32(self.dt_seconds), self.d_il, self.d_xl, self.tan2,
+                       self.dt_seconds)
+
+
+def plan_geometry(n_il: int, n_xl: int, n_t: int, dt_seconds: float, d_il: float,
+                  d_xl: float, angle: float, max_v: float, pad_il: int = 0, pad_xl: int = 0,
+                  amp: bool = True, il_labels=None, xl_labels=None,
+                  precision: str = "f32") -> Geometry:
+    """Geometry of a migration as src/main.cpp:140-217 derives it.  max_v is the value of
+    estimateMaxVelocity (main.cpp:22-64)."""
+    il_labels = np.arange(1, n_il + 1) if il_labels is None else np.asarray(il_labels)
+    xl_labels = np.arange(1, n_xl + 1) if xl_labels is None else np.asarray(xl_labels)
+    out_il = padded_labels(il_labels, pad_il)
+    out_xl = padded_labels(xl_labels, pad_xl)
+    t2 = tan2_theta(angle)
+    return Geometry(n_il, n_xl, n_t, dt_seconds, d_il, d_xl, t2,
+                    max_aperture_il(max_v if max_v >= 100.0 else 3000.0, n_t, dt_seconds, t2,
+                                    d_il),
+                    pad_il, pad_xl, len(out_il), len(out_xl),
+                    output_centers(il_labels, out_il), amp, precision)
+
+
+def estimate_max_velocity(vrms: np.ndarray) -> float:
+    """src/main.cpp:22-64 on a dense Vrms cube: max over (first, middle, last) inline x
+    (first, middle, last) crossline at the last sample; below 100 m/s -> 3000."""
+    n_il, n_xl, n_t = vrms.shape
+    ils = [0] + ([n_il // 2, n_il - 1] if n_il > 1 else [])
+    xls = [0] + ([n_xl // 2, n_xl - 1] if n_xl > 1 else [])
+    mv = 0.0
+    for i in ils:
+        for x in xls:
+            mv = max(mv, float(vrms[i, x, n_t - 1]))
+    return mv if mv >= 100.0 else 3000.0
+
+
+# ----------------------------------------------------------------------------- operator
+
+
+class Migrator:
+    """A cube resident on one GPU and its forward (migration) operator."""
+
+    def __init__(self, device: int = 0):
+        self._L = _lib.cuda()
+        self._ctx = ctypes.c_void_p()
+        check(self._L.psm_create(ctypes.byref(self._ctx), device), lambda: "psm_create")
+        self.geom: Optional[Geometry] = None
+
+    def _err(self):
+        return self._L.psm_last_error(self._ctx).decode()
+
+    def close(self):
+        if self._ctx:
+            self._L.psm_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_geometry(self, g: Geometry) -> None:
+        oc = np.ascontiguousarray(g.out_center, dtype=np.int32)
+        gc = g.to_c()
+        check(self._L.psm_set_geometry(self._ctx, ctypes.byref(gc), oc.ctypes.data),
+              self._err)
+        self.geom = g
+
+    def set_traces(self, data) -> None:
+        g = self.geom
+        if isinstance(data, np.ndarray):
+            data = _f32(data, (g.n_il, g.n_xl, g.n_t))
+        check(self._L.psm_set_traces(self._ctx, _addr(data)), self._err)
+
+    def set_vrms(self, vrms) -> None:
+        g = self.geom
+        if isinstance(vrms, np.ndarray):
+            vrms = _f32(vrms, (g.n_il, g.n_xl, g.n_t))
+        check(self._L.psm_set_vrms(self._ctx, _addr(vrms)), self._err)
+
+    def image_shape(self):
+        g = self.geom
+        return (g.n_oi, g.n_ox, g.n_t)
+
+    def forward(self, out=None):
+        """Migrate the resident cube; returns image [n_oi][n_ox][n_t] (host)."""
+        if out is None:
+            out = np.empty(self.image_shape(), dtype=np.float32)
+        check(self._L.psm_forward(self._ctx, _addr(out)), self._err)
+        return out
+
+    def forward_async(self) -> None:
+        check(self._L.psm_forward_async(self._ctx), self._err)
+
+    def synchronize(self) -> None:
+        check(self._L.psm_synchronize(self._ctx), self._err)
+
+    def get_image(self, out=None):
+        if out is None:
+            out = np.empty(self.image_shape(), dtype=np.float32)
+        check(self._L.psm_get_image(self._ctx, _addr(out)), self._err)
+        return out
+
+    def image_device_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        check(self._L.psm_image_device(self._ctx, ctypes.byref(p)), self._err)
+        return p.value
+
+    def stream_handle(self) -> int:
+        p = ctypes.c_void_p()
+        check(self._L.psm_stream(self._ctx, ctypes.byref(p)), self._err)
+        return p.value or 0
+
+    def count_terms(self) -> int:
+        """Terms that pass every reference mask over the real input traces, all output
+        inlines (padded ones included)."""
+        n = ctypes.c_int64()
+        check(self._L.psm_count_terms(self._ctx, ctypes.byref(n)), self._err)
+        return int(n.value)
+
+    def count_terms_rows(self) -> np.ndarray:
+        out = np.zeros(self.geom.n_oi, dtype=np.int64)
+        check(self._L.psm_count_terms_rows(self._ctx, out.ctypes.data), self._err)
+        return out
+
+
+class MigrationKernel:
+    """Mirror of the reference's static class MigrationKernel (include/migration_kernel.h)."""
+
+    @staticmethod
+    def kirchhoff_kernel_3d_with_padding(input_buffer, n_buf_il, n_buf_xl, n_t,
+                                         velocity_slice, output_slice, il_pos_indices,
+                                         xl_pos_indices, current_il_pos, current_xl_start,
+                                         dt, t0_times, tan_theta_sq, inline_bin_size,
+                                         crossline_bin_size, amp_correction):
+        """kirchhoffKernel3DWithPadding on the GPU.  output_slice: float32 array
+        [n_out_xl][n_t], fully overwritten in place (as the reference overwrites its
+        vector<vector<float>>)."""
+        L = _lib.cuda()
+        buf = _f32(input_buffer).reshape(-1)
+        vel = _f32(velocity_slice).reshape(-1)
+        if buf.size != n_buf_il * n_buf_xl * n_t:
+            raise ValueError("input_buffer size mismatch")
+        if vel.size < n_buf_xl * n_t:
+            raise ValueError("velocity_slice size mismatch")
+        if not (isinstance(output_slice, np.ndarray) and output_slice.dtype == np.float32
+                and output_slice.flags["C_CONTIGUOUS"]):
+            raise TypeError("output_slice must be a C-contiguous float32 array")
+        n_out_xl = output_slice.shape[0] if output_slice.ndim > 1 else (
+            output_slice.size // max(n_t, 1))
+        ilp = np.ascontiguousarray(il_pos_indices, dtype=np.int32)
+        t0 = _f32(t0_times)
+        if t0.size < n_t:
+            raise ValueError("t0_times shorter than n_t")
+        rc = L.psm_kirchhoff_inline(buf.ctypes.data, n_buf_il, n_buf_xl, n_t, vel.ctypes.data,
+                                    output_slice.ctypes.data, n_out_xl, ilp.ctypes.data, None,
+                                    int(current_il_pos), int(current_xl_start),
+                                    np.float32(dt), t0.ctypes.data, np.float32(tan_theta_sq),
+                                    np.float32(inline_bin_size),
+                                    np.float32(crossline_bin_size), int(bool(amp_correction)))
+        check(rc, lambda: L.psm_kirchhoff_inline_error().decode())
+        return output_slice
