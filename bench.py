@@ -49,7 +49,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["config2", "config1"], default="config2")
+    p.add_argument("--workload", choices=["config2", "config2_201", "config1"],
+                   default="config2")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     p.add_argument("--cpu-rows", type=int, default=2,
                    help="output inlines in the bounded CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -58,7 +60,11 @@ def parse():
 
 def workload(name):
     from poststackmig3d_b200 import synth as S
-    return S.workload_config2() if name == "config2" else S.workload_config1()
+    if name == "config2":
+        return S.workload_config2()
+    if name == "config2_201":  # same recipe on 201x201 traces: the profiling case
+        return S.workload_config2(n=201)
+    return S.workload_config1()
 
 
 def geometry(W):
@@ -303,31 +309,36 @@ def run_ours(args):
     value = world * n_terms / (ms_max * 1e-3) / 1e9
 
     # ---- end to end through the public API: pinned host inputs -> image on the host
-    h_data = torch.from_numpy(W.data).pin_memory()
-    h_vrms = torch.from_numpy(W.vrms_cube()).pin_memory()
-    h_img = torch.empty(m.image_shape(), dtype=torch.float32).pin_memory()
-    e2e_steps = max(1, min(args.steps, 3))
-    m.set_traces(h_data)
-    m.set_vrms(h_vrms)
-    m.forward(h_img)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
+    e2e = None
+    if not args.no_e2e:
+        h_data = torch.from_numpy(W.data).pin_memory()
+        h_vrms = torch.from_numpy(W.vrms_cube()).pin_memory()
+        h_img = torch.empty(m.image_shape(), dtype=torch.float32).pin_memory()
+        e2e_steps = max(1, min(args.steps, 3))
         m.set_traces(h_data)
         m.set_vrms(h_vrms)
         m.forward(h_img)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n_terms / (e2e_ms * 1e-3) / 1e9
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            m.set_traces(h_data)
+            m.set_vrms(h_vrms)
+            m.forward(h_img)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / e2e_steps
+        if dist:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * n_terms / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+               "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": int(h_data.numel() * 4 + h_vrms.numel() * 4),
+               "d2h_bytes_per_step": int(h_img.numel() * 4)}
 
     clocks = clk.summary()
     sm_mhz = clocks["sm_mhz"] or 1965.0
@@ -367,10 +378,7 @@ def run_ours(args):
                 "dtype": "f32", "data": "synthetic (seeded)",
                 "config": config_dict(W, g, {"n_terms": n_terms,
                                              "parallelism": f"replicas x{world}"}),
-                "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": UNIT,
-                        "h2d_bytes_per_step": int(h_data.numel() * 4 + h_vrms.numel() * 4),
-                        "d2h_bytes_per_step": int(h_img.numel() * 4)},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": args.steps, "clocks": clocks}
         print(json.dumps(line), flush=True)
     m.close()

@@ -22,7 +22,7 @@ typedef struct {
 } point_t;
 
 static point_t point_setup(float t0v, float v, float tan2, float inv_dxl, int64_t xb,
-                           int64_t n_buf_xl) {
+                           int64_t n_buf_xl, int contract) {
     point_t p;
     memset(&p, 0, sizeof p);
     if (!(v >= 1e-5f && t0v >= 1e-5f)) return p; /* :121 */
@@ -30,7 +30,8 @@ static point_t point_setup(float t0v, float v, float tan2, float inv_dxl, int64_
     p.t0sq = t0v * t0v;                           /* :125 */
     p.v = v;
     float vsq = v * v;                            /* :127 */
-    float inv_vsq = 1.0f / (vsq + 1e-10f);        /* :128 */
+    /* :128; the reference's build fuses v*v + 1e-10 */
+    float inv_vsq = 1.0f / (contract ? fmaf(v, v, 1e-10f) : vsq + 1e-10f);
     p.f4 = 4.0f * inv_vsq;                        /* :129 */
     float vth = v * t0v * 0.5f;                   /* :133 */
     p.maxd2 = vth * vth * tan2;                   /* :134 */
@@ -115,7 +116,7 @@ static void trace_forward(const src_t *src, int64_t n_buf_il, int64_t n_buf_xl, 
     const float inv_dxl = 1.0f / d_xl;          /* :45 */
     for (int64_t t = 0; t < n_t; ++t) {
         float v = vel_x ? vel_x[t] : 0.0f;
-        point_t p = point_setup(t0[t], v, tan2, inv_dxl, xb, n_buf_xl);
+        point_t p = point_setup(t0[t], v, tan2, inv_dxl, xb, n_buf_xl, contract);
         if (!p.valid) { /* :148-151 */
             if (o32) o32[t] = 0.0f;
             if (o64) o64[t] = 0.0;
@@ -289,7 +290,7 @@ void oracle_count_rows(const float *vrms, int32_t n_il, int32_t n_xl, int32_t n_
             if (xb >= n_buf_xl || xc < 0 || xc >= n_xl) continue;
             const float *vel_x = vrms + ((int64_t)c * n_xl + xc) * n_t;
             for (int64_t t = 0; t < n_t; ++t) {
-                point_t p = point_setup(t0[t], vel_x[t], tan2, inv_dxl, xb, n_buf_xl);
+                point_t p = point_setup(t0[t], vel_x[t], tan2, inv_dxl, xb, n_buf_xl, contract);
                 if (!p.valid) continue;
                 for (int32_t il = il0; il < il1; ++il) {
                     float dx = (float)(il - c) * d_il;
@@ -340,7 +341,7 @@ void oracle_adjoint_volume(const double *image, const float *vrms, int32_t n_il,
             if (xc < 0 || xc >= n_xl) continue; /* v = 0 there: no terms */
             const float *vel_x = vrms + ((int64_t)c * n_xl + xc) * n_t;
             for (int64_t t = 0; t < n_t; ++t) {
-                point_t p = point_setup(t0[t], vel_x[t], tan2, inv_dxl, xb, n_buf_xl);
+                point_t p = point_setup(t0[t], vel_x[t], tan2, inv_dxl, xb, n_buf_xl, contract);
                 if (!p.valid) continue;
                 double m = image[((int64_t)o * n_ox + xb) * n_t + t];
                 if (m == 0.0) continue;

@@ -102,6 +102,7 @@ void fill_consts(FwdParams& P, float dt, float d_il, float d_xl, float tan2) {
     P.tan2 = tan2;
     P.tanth = std::sqrt(std::max(tan2, 0.0f));
     P.ntm1f = static_cast<float>(P.n_t) - 1.0f;
+    P.ntm1m = std::nextafter(P.ntm1f, 0.0f);
 }
 
 }  // namespace

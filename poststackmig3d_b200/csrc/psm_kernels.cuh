@@ -56,7 +56,9 @@ struct FwdParams {
     int n_vx;             // crosslines of a Vrms plane
     int n_ox;             // output crosslines per row
     int xoff;             // cube / Vrms crossline of output x is x + xoff
-    float inv_dt, idt2, d_il, d_xl, inv_dxl, tan2, tanth, ntm1f;
+    float inv_dt, idt2, d_il, d_xl, inv_dxl, tan2, tanth;
+    float ntm1f;  // n_t - 1
+    float ntm1m;  // largest float below n_t - 1
 };
 
 struct StageMeta {
@@ -156,16 +158,42 @@ struct PointConst {
     float t0sq, f4, md2, vsq;
 };
 
+// The reference's build (GCC, -ffp-contract=fast) fuses v*v + 1e-10 into one fma.
 __device__ __forceinline__ PointConst point_const(float v, float t0v, float tan2) {
     PointConst p;
-    p.valid = (v >= 1e-5f) && (t0v >= 1e-5f);                 // :121
-    p.t0sq = __fmul_rn(t0v, t0v);                              // :125
-    p.vsq = __fmul_rn(v, v);                                   // :127
-    float inv_vsq = __fdiv_rn(1.0f, __fadd_rn(p.vsq, 1e-10f)); // :128
-    p.f4 = __fmul_rn(4.0f, inv_vsq);                           // :129
-    float vth = __fmul_rn(__fmul_rn(v, t0v), 0.5f);            // :133
-    p.md2 = __fmul_rn(__fmul_rn(vth, vth), tan2);              // :134
+    p.valid = (v >= 1e-5f) && (t0v >= 1e-5f);                       // :121
+    p.t0sq = __fmul_rn(t0v, t0v);                                    // :125
+    p.vsq = __fmul_rn(v, v);                                         // :127
+    float inv_vsq = __fdiv_rn(1.0f, __fmaf_rn(v, v, 1e-10f));        // :128
+    p.f4 = __fmul_rn(4.0f, inv_vsq);                                 // :129
+    float vth = __fmul_rn(__fmul_rn(v, t0v), 0.5f);                  // :133
+    p.md2 = __fmul_rn(__fmul_rn(vth, vth), tan2);                    // :134
     return p;
+}
+
+// The reference keeps a term when floor(s) < n_t - 1 with s = fl(sqrt(fma(f4, r2, t0^2)) *
+// inv_dt) in IEEE FP32 (migration_kernel.cpp:209-226, :291-298).  s grows monotonically
+// with r2, so the kept r2 form a prefix [0, R].  Return B = min(md2, R): a term passes both
+// of the reference's masks exactly when r2 <= B (B < 0: no term passes).  Found by bisection
+// on the bit patterns of the non-negative floats in [0, md2] with the reference arithmetic.
+__device__ __forceinline__ bool range_ok(float r2, float f4, float t0sq, float inv_dt,
+                                         float ntm1f) {
+    return __fmul_rn(__fsqrt_rn(__fmaf_rn(f4, r2, t0sq)), inv_dt) < ntm1f;
+}
+
+__device__ __forceinline__ float pass_bound(const PointConst& p, float inv_dt, float ntm1f) {
+    if (!p.valid || !(p.md2 >= 0.0f)) return -1.0f;
+    if (range_ok(p.md2, p.f4, p.t0sq, inv_dt, ntm1f)) return p.md2;
+    if (!range_ok(0.0f, p.f4, p.t0sq, inv_dt, ntm1f)) return -1.0f;
+    unsigned lo = 0u, hi = __float_as_uint(p.md2);  // ok(lo), !ok(hi)
+    while (hi - lo > 1u) {
+        const unsigned mid = lo + ((hi - lo) >> 1);
+        if (range_ok(__uint_as_float(mid), p.f4, p.t0sq, inv_dt, ntm1f))
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return __uint_as_float(lo);
 }
 
 // dx^2 of a buffer inline (migration_kernel.cpp:51-56).
@@ -253,14 +281,15 @@ __global__ void __launch_bounds__(32 * (kTX + 1))
                 t0v = __ldg(P.t0 + t);
             }
             PointConst pc = point_const(v, t0v, P.tan2);
+            const float bnd = pass_bound(pc, P.inv_dt, P.ntm1f);
             acc[j] = 0.0f;
-            if (pc.valid) {
+            if (bnd >= 0.0f) {
                 t02s[j] = pc.t0sq * P.idt2;
                 f4s[j] = pc.f4 * P.idt2;
-                md2s[j] = pc.md2;
+                md2s[j] = bnd;
                 vmin = fminf(vmin, v);
                 vmax = fmaxf(vmax, v);
-                md2max = fmaxf(md2max, pc.md2);
+                md2max = fmaxf(md2max, bnd);
                 t0min = fminf(t0min, t0v);
                 t0max = fmaxf(t0max, t0v);
             } else {
@@ -413,10 +442,11 @@ __global__ void __launch_bounds__(32 * (kTX + 1))
 #pragma unroll
             for (int j = 0; j < J; ++j) {
                 if (r2 > blkmax[j]) continue;
-                const float t2 = __fmaf_rn(f4s[j], r2, t02s[j]);  // (t / dt)^2
-                const float q = rsqrtf(t2);                        // dt / t
-                const float s = t2 * q;                            // t / dt
-                if (r2 <= md2s[j] && s < P.ntm1f) {
+                if (r2 <= md2s[j]) {  // both reference masks, exactly (pass_bound)
+                    const float t2 = __fmaf_rn(f4s[j], r2, t02s[j]);  // (t / dt)^2
+                    const float q = rsqrtf(t2);                        // dt / t
+                    // t / dt; the reference's s is < n_t - 1 here, keep ours below it too
+                    const float s = fminf(t2 * q, P.ntm1m);
                     const float mm = __fadd_rd(s, 8388608.0f);
                     const int lo = __float_as_int(mm) - 0x4B000000;  // floor(s)
                     const float fr = s - (mm - 8388608.0f);
@@ -466,18 +496,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1))
 
 // ----------------------------------------------------------------------------- term count
 
-// Largest crossline distance d >= 0 whose term passes both masks for this output sample,
-// or -1.  Both masks are monotone in r^2, so the passing crosslines are |k - x| <= d.
-__device__ __forceinline__ bool term_pass(int d, float d_xl, float dx2, float md2, float f4s,
-                                          float t02s, float ntm1f) {
-    const float r2 = trace_r2(d, d_xl, dx2);
-    if (!(r2 <= md2)) return false;
-    const float t2 = __fmaf_rn(f4s, r2, t02s);
-    const float s = t2 * rsqrtf(t2);
-    return s < ntm1f;
-}
-
 // One block per (job, output crossline); threads stride over t.  out[job] += terms.
+// A term passes when r^2 <= B (pass_bound); r^2 grows with |k - x|, so for each buffer
+// inline the passing crosslines are |k - x| <= d with d found from sqrt(B - dx^2) and exact
+// fix-ups.
 __global__ void count_kernel(const FwdParams P, unsigned long long* out) {
     __shared__ unsigned long long wsum[32];
     const int x = blockIdx.x;
@@ -488,24 +510,15 @@ __global__ void count_kernel(const FwdParams P, unsigned long long* out) {
         if (xv < 0 || xv >= P.n_vx) break;
         const float v = P.vrms[(static_cast<size_t>(job.vrow) * P.n_vx + xv) * P.n_t + t];
         const PointConst pc = point_const(v, P.t0[t], P.tan2);
-        if (!pc.valid) continue;
-        const float f4s = pc.f4 * P.idt2, t02s = pc.t0sq * P.idt2;
+        const float B = pass_bound(pc, P.inv_dt, P.ntm1f);
+        if (B < 0.0f) continue;
         for (int i = job.i0; i < job.i1; ++i) {
             const float dx2 = inline_dx2(P.il_pos[i], job.pos, P.d_il);
-            if (dx2 > pc.md2) continue;
-            if (!term_pass(0, P.d_xl, dx2, pc.md2, f4s, t02s, P.ntm1f)) continue;
-            int d = static_cast<int>(sqrtf(fmaxf(pc.md2 - dx2, 0.0f)) * P.inv_dxl);
-            // the range mask: t^2 < ntm1^2 -> r^2 < (ntm1^2 - t02s) / f4s
-            if (f4s > 0.0f) {
-                const float r2s = (P.ntm1f * P.ntm1f - t02s) / f4s - dx2;
-                if (r2s <= 0.0f)
-                    d = 0;
-                else
-                    d = min(d, static_cast<int>(sqrtf(r2s) * P.inv_dxl) + 1);
-            }
+            if (dx2 > B) continue;  // d = 0 passes from here on
+            int d = static_cast<int>(sqrtf(fmaxf(B - dx2, 0.0f)) * P.inv_dxl);
             d = min(d, P.n_cx + 1);
-            while (d > 0 && !term_pass(d, P.d_xl, dx2, pc.md2, f4s, t02s, P.ntm1f)) --d;
-            while (d <= P.n_cx && term_pass(d + 1, P.d_xl, dx2, pc.md2, f4s, t02s, P.ntm1f)) ++d;
+            while (d > 0 && trace_r2(d, P.d_xl, dx2) > B) --d;
+            while (d <= P.n_cx && trace_r2(d + 1, P.d_xl, dx2) <= B) ++d;
             const int lo = max(0, xv - d), hi = min(P.n_cx - 1, xv + d);
             if (hi >= lo) local += static_cast<unsigned long long>(hi - lo + 1);
         }
