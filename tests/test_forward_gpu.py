@@ -10,7 +10,8 @@ import oracle as O
 from poststackmig3d_b200 import synth as S
 from poststackmig3d_b200 import MigrationKernel, Migrator, plan_geometry
 
-from helpers import MAX_REL_TOL, REL_RMS_TOL, geometry_for, gpu_forward, oracle_forward, rel_err
+from helpers import (MAX_REL_TOL, REL_RMS_TOL, fp32_floor_ok, geometry_for, gpu_forward,
+                     oracle_forward, rel_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -35,6 +36,9 @@ def test_forward_matches_oracle(case):
     ref, _, counts = oracle_forward(W, g)
     rms, mx = rel_err(img, ref)
     assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (rms, mx)
+    _, ref64, _ = oracle_forward(W, g, O.CONTRACT | O.F64, want64=True)
+    ok, errs = fp32_floor_ok(img, ref, ref64)
+    assert ok, errs
     # real-trace terms: the kernel's masks are the reference's FP32 arithmetic exactly
     assert n_gpu == counts[1], (n_gpu, counts)
 
@@ -47,6 +51,9 @@ def test_config1_full_size():
     ref, _, counts = oracle_forward(W, g)
     rms, mx = rel_err(img, ref)
     assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (rms, mx)
+    _, ref64, _ = oracle_forward(W, g, O.CONTRACT | O.F64, want64=True)
+    ok, errs = fp32_floor_ok(img, ref, ref64)
+    assert ok, errs
     assert counts[0] == 2855016288  # all accumulated terms, zero padding traces included
     assert n_gpu == counts[1] == 2672050496  # terms on real input traces
     # padded output inlines repeat the edge inlines; padded crosslines are zero
