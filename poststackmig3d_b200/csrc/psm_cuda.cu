@@ -18,15 +18,20 @@ namespace {
 using psm::FwdParams;
 using psm::Job;
 
-constexpr size_t kFwdSmem =
-    ((sizeof(uint64_t) * 2 * psm::kStages + sizeof(psm::StageMeta) * psm::kStages +
-      sizeof(psm::TileStats) * psm::kTX + 127) &
-     ~size_t(127)) +
-    sizeof(float) * psm::kStages * psm::kStageCap;
+constexpr size_t kMaxDynSmem = 232448;  // 227 KB per CTA on sm_100
 
-// Trace stride in HBM: n_t rounded up to 8 samples (32 B) so every trace starts 16 B aligned
-// for the TMA bulk copies; the tail samples stay zero.
+// Trace stride in HBM: n_t rounded up to 8 samples so every trace starts 32 B aligned for
+// the TMA bulk copies; the tail samples stay zero.
 inline int trace_stride(int n_t) { return (n_t + 7) & ~7; }
+
+// Ring stage capacity (samples): at least one whole trace so a stage always takes a window.
+inline int stage_cap(int ns) { return std::max(psm::kStageCapMin, ns); }
+
+int max_inline_window(const std::vector<Job>& jobs) {
+    int m = 1;
+    for (const Job& j : jobs) m = std::max(m, j.i1 - j.i0);
+    return m;
+}
 
 struct DevBuf {
     void* p = nullptr;
@@ -66,31 +71,41 @@ struct Status {
                              std::string(#call) + ": " + cudaGetErrorString(e_));        \
     } while (0)
 
-// Launch the forward kernel for n_jobs jobs (template dispatch on J and amplitude mode).
-template <int J>
-cudaError_t launch_fwd_j(const FwdParams& P, int n_jobs, bool amp, cudaStream_t s) {
-    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + 32 * J - 1) / (32 * J), n_jobs);
+// Dynamic shared memory of a forward launch (0: too large for one CTA).
+size_t fwd_smem(const FwdParams& P) {
+    const size_t b = psm::smem_layout(P.max_inl, P.stage_cap).total;
+    return b <= kMaxDynSmem ? b : 0;
+}
+
+// Launch the forward kernel for n_jobs jobs (P.max_inl and P.stage_cap set).
+cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, cudaStream_t s) {
+    if (n_jobs <= 0 || P.n_ox <= 0 || P.n_t <= 0) return cudaSuccess;
+    const size_t smem = fwd_smem(P);
+    if (!smem) return cudaErrorInvalidValue;
+    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + psm::kTT - 1) / psm::kTT, n_jobs);
     dim3 block(32 * (psm::kTX + 1));
     cudaError_t e;
     if (amp) {
-        e = cudaFuncSetAttribute(psm::fwd_kernel<J, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
+        e = cudaFuncSetAttribute(psm::fwd_kernel<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        psm::fwd_kernel<J, true><<<grid, block, kFwdSmem, s>>>(P);
+        psm::fwd_kernel<true><<<grid, block, smem, s>>>(P);
     } else {
-        e = cudaFuncSetAttribute(psm::fwd_kernel<J, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
+        e = cudaFuncSetAttribute(psm::fwd_kernel<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        psm::fwd_kernel<J, false><<<grid, block, kFwdSmem, s>>>(P);
+        psm::fwd_kernel<false><<<grid, block, smem, s>>>(P);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, cudaStream_t s) {
-    if (n_jobs <= 0 || P.n_ox <= 0 || P.n_t <= 0) return cudaSuccess;
-    if (P.n_t <= 64) return launch_fwd_j<2>(P, n_jobs, amp, s);
-    if (P.n_t <= 128) return launch_fwd_j<4>(P, n_jobs, amp, s);
-    return launch_fwd_j<8>(P, n_jobs, amp, s);
+// pairs[n_rows][ns] from the fp32 rows (pair_kernel).
+cudaError_t build_pairs(const float* src, float2* dst, size_t n_rows, int ns, cudaStream_t s) {
+    if (!n_rows) return cudaSuccess;
+    const size_t n = n_rows * static_cast<size_t>(ns);
+    const unsigned blocks = static_cast<unsigned>(std::min<size_t>((n + 255) / 256, 148 * 64));
+    psm::pair_kernel<<<blocks, 256, 0, s>>>(src, dst, n_rows, ns);
+    return cudaGetLastError();
 }
 
 void fill_consts(FwdParams& P, float dt, float d_il, float d_xl, float tan2) {
@@ -119,14 +134,16 @@ struct psm_ctx {
     std::vector<Job> jobs;       // one per distinct migrated inline
     std::vector<Job> jobs_all;   // one per output row (term counting)
     std::vector<std::pair<int, int>> copies;  // (dst row, src row) duplicated output rows
-    DevBuf data, vrms, image, d_jobs, d_jobs_all, il_pos, t0, err, count;
+    // data: fp32 traces [n_il][n_xl][ns] as uploaded; pairs: the (d, d[t+1]-d) cube the
+    // forward kernel stages
+    DevBuf data, pairs, vrms, image, d_jobs, d_jobs_all, il_pos, t0, err, count;
 };
 
 namespace {
 
 FwdParams volume_params(psm_ctx* c) {
     FwdParams P{};
-    P.data = c->data.as<float>();
+    P.pairs = c->pairs.as<float2>();
     P.vrms = c->vrms.as<float>();
     P.image = c->image.as<float>();
     P.jobs = c->d_jobs.as<Job>();
@@ -140,6 +157,8 @@ FwdParams volume_params(psm_ctx* c) {
     P.n_vx = c->g.n_xl;
     P.n_ox = c->g.n_ox;
     P.xoff = -c->g.pad_xl;
+    P.max_inl = max_inline_window(c->jobs_all);
+    P.stage_cap = stage_cap(c->ns);
     fill_consts(P, c->g.dt, c->g.d_il, c->g.d_xl, c->g.tan2_theta);
     return P;
 }
@@ -188,6 +207,7 @@ int psm_destroy(psm_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->data.release();
+    c->pairs.release();
     c->vrms.release();
     c->image.release();
     c->d_jobs.release();
@@ -219,8 +239,11 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
     if (g->precision != PSM_F32)
         return c->st.fail(PSM_ERR_UNSUPPORTED, "only PSM_F32 storage is built");
     const int ns = trace_stride(g->n_t);
-    if (ns > psm::kStageCap)
-        return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t too large for the staging ring");
+    // inline window of any output inline <= 2 (m_il + pad_il) + 1 (+ the inline table) and one
+    // whole trace per ring stage must fit the CTA's shared memory
+    const int64_t win = std::min<int64_t>(g->n_il, 2 * (int64_t(g->m_il) + g->pad_il) + 1);
+    if (psm::smem_layout(static_cast<int>(win), stage_cap(ns)).total > kMaxDynSmem)
+        return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t / aperture too large for the staging ring");
     std::vector<int> center(g->n_oi);
     for (int o = 0; o < g->n_oi; ++o) {
         int cc = out_center ? out_center[o] : std::min(std::max(o - g->pad_il, 0), g->n_il - 1);
@@ -254,6 +277,7 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
     const size_t n_tr = static_cast<size_t>(g->n_il) * g->n_xl;
     PSM_CUDA_TRY(c->st, c->data.ensure(n_tr * ns * sizeof(float)));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->data.p, 0, n_tr * ns * sizeof(float), c->stream));
+    PSM_CUDA_TRY(c->st, c->pairs.ensure(n_tr * ns * sizeof(float2)));
     PSM_CUDA_TRY(c->st, c->vrms.ensure(n_tr * g->n_t * sizeof(float)));
     PSM_CUDA_TRY(c->st, c->image.ensure(static_cast<size_t>(g->n_oi) * g->n_ox * g->n_t *
                                         sizeof(float)));
@@ -290,6 +314,8 @@ int psm_set_traces(psm_ctx* c, const float* data) {
     PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.p, c->ns * sizeof(float), data,
                                           c->g.n_t * sizeof(float), c->g.n_t * sizeof(float),
                                           n_tr, cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>(), c->pairs.as<float2>(), n_tr, c->ns,
+                                    c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     c->have_traces = true;
     return PSM_OK;
@@ -399,7 +425,7 @@ struct InlineStaging {
     int device = -1;
     cudaStream_t stream = nullptr;
     Status st;
-    DevBuf data, vel, out, job, il_pos, t0, err;
+    DevBuf data, pairs, vel, out, job, il_pos, t0, err;
     ~InlineStaging() {
         if (stream) cudaStreamDestroy(stream);
     }
@@ -428,8 +454,9 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
         return PSM_ERR_ARG;
     }
     const int ns = trace_stride(static_cast<int>(n_t));
-    if (ns > psm::kStageCap) {
-        tl_inline_error = "n_t too large for the staging ring";
+    if (psm::smem_layout(std::max<int>(static_cast<int>(n_buf_il), 1), stage_cap(ns)).total >
+        kMaxDynSmem) {
+        tl_inline_error = "n_t / buffer too large for the staging ring";
         return PSM_ERR_UNSUPPORTED;
     }
     if (!tl_staging) tl_staging.reset(new (std::nothrow) InlineStaging());
@@ -456,6 +483,7 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
     }
     const size_t n_tr = n_buf_il * n_buf_xl;
     PSM_INL_TRY(S->data.ensure(std::max<size_t>(n_tr, 1) * ns * sizeof(float)));
+    PSM_INL_TRY(S->pairs.ensure(std::max<size_t>(n_tr, 1) * ns * sizeof(float2)));
     PSM_INL_TRY(S->vel.ensure(std::max<size_t>(n_buf_xl, 1) * n_t * sizeof(float)));
     PSM_INL_TRY(S->out.ensure(n_out_xl * n_t * sizeof(float)));
     PSM_INL_TRY(S->job.ensure(sizeof(Job)));
@@ -468,6 +496,7 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
         PSM_INL_TRY(cudaMemcpy2DAsync(S->data.p, ns * sizeof(float), input_buffer,
                                       n_t * sizeof(float), n_t * sizeof(float), n_tr,
                                       cudaMemcpyHostToDevice, s));
+        PSM_INL_TRY(build_pairs(S->data.as<float>(), S->pairs.as<float2>(), n_tr, ns, s));
     }
     if (n_buf_xl)
         PSM_INL_TRY(cudaMemcpyAsync(S->vel.p, velocity_slice, n_buf_xl * n_t * sizeof(float),
@@ -485,7 +514,7 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
     PSM_INL_TRY(cudaMemcpyAsync(S->job.p, &j, sizeof(Job), cudaMemcpyHostToDevice, s));
     PSM_INL_TRY(cudaMemsetAsync(S->err.p, 0, sizeof(int), s));
     FwdParams P{};
-    P.data = S->data.as<float>();
+    P.pairs = S->pairs.as<float2>();
     P.vrms = S->vel.as<float>();
     P.image = S->out.as<float>();
     P.jobs = S->job.as<Job>();
@@ -499,6 +528,8 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
     P.n_vx = static_cast<int>(n_buf_xl);
     P.n_ox = static_cast<int>(n_out_xl);
     P.xoff = current_xl_start;
+    P.max_inl = std::max<int>(static_cast<int>(n_buf_il), 1);
+    P.stage_cap = stage_cap(ns);
     fill_consts(P, dt, inline_bin_size, crossline_bin_size, tan_theta_sq);
     PSM_INL_TRY(launch_fwd(P, 1, amp_correction != 0, s));
     PSM_INL_TRY(cudaMemcpyAsync(output_slice, S->out.p, n_out_xl * n_t * sizeof(float),

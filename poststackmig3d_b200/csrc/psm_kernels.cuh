@@ -7,17 +7,23 @@
 // with t = sqrt(t0^2 + 4 r^2 / v^2), v the output point's Vrms, interp the linear rule
 // fma(frac, d[lo+1] - d[lo], d[lo]) (simdInterpolate, :544-550).
 //
+// HBM layout: the traces are held as a "pair cube" [inline][crossline][ns] of float2
+// (d[t], d[t+1] - d[t]) built once after upload (pair_kernel), so one 8-byte shared-memory
+// load gives both interpolation operands with the reference's own difference.
+//
 // Work decomposition (one CTA):
-//   * one output row ("job": an output inline), TX consecutive output crosslines, TT
-//     consecutive output samples (a "tile");
-//   * warp 0 is the producer: it enumerates the input traces that can reach the tile, derives
-//     for each a time window [ws, we) that covers every unmasked term of the tile, and stages
-//     the windows into shared memory with TMA bulk copies (cp.async.bulk) into a ring of
-//     kStages buffers guarded by mbarriers;
-//   * warps 1..TX are consumers: warp w owns output crossline x0 + w-1 and holds, per lane,
-//     J samples t0 = T0 + lane + 32 j.  For each staged trace the per-trace quantities
-//     (dy, r^2, window base) are warp-uniform; each lane evaluates its J terms from shared
-//     memory.
+//   * one output row ("job": an output inline), kTX consecutive output crosslines and
+//     kTT = 256 consecutive output samples (a "tile");
+//   * warp 0 is the producer: it lists the input traces that can reach the tile, derives for
+//     each a window [ws, we) of samples that covers every term of the tile that passes the
+//     masks, and stages the windows into shared memory with TMA bulk copies (cp.async.bulk)
+//     into a ring of kStages buffers guarded by mbarriers;
+//   * warps 1..kTX are consumers: warp w owns output crossline x0 + w - 1; lane l holds the
+//     8 samples t0 = T0 + l + 32 j (j = 0..7) as 4 register pairs, evaluated with packed
+//     f32x2 arithmetic.  Per staged trace the quantities dy, r^2 and the window base are
+//     warp-uniform.
+// Masks: a term passes the reference's aperture and range masks exactly when r^2 <= B, B a
+// per-sample bound found once with the reference's IEEE arithmetic (pass_bound).
 // Every wait is bounded: on expiry the kernel records PSM_DEV_ERR_TIMEOUT in *err and leaves.
 #pragma once
 
@@ -26,11 +32,13 @@
 
 namespace psm {
 
-constexpr int kTX = 8;            // output crosslines per CTA (one consumer warp each)
-constexpr int kStages = 2;        // TMA ring depth
-constexpr int kStageCap = 12288;  // floats per ring stage (48 KB)
-constexpr int kMaxG = 32;         // traces per ring stage
-constexpr unsigned kWaitLimit = 1u << 26;  // bounded mbarrier polls
+constexpr int kTX = 8;          // output crosslines per CTA (one consumer warp each)
+constexpr int kJ = 8;           // 32-sample blocks per consumer lane
+constexpr int kTT = 32 * kJ;    // output samples per CTA
+constexpr int kStages = 2;      // TMA ring depth
+constexpr int kMaxG = 32;       // traces per ring stage
+constexpr int kStageCapMin = 6144;          // samples (8 B each) per ring stage, at least
+constexpr unsigned kWaitLimit = 1u << 26;   // bounded mbarrier polls
 
 constexpr int PSM_DEV_ERR_TIMEOUT = 1;
 constexpr int PSM_DEV_ERR_WINDOW = 2;  // debug-bounds build only
@@ -45,8 +53,8 @@ struct Job {
 };
 
 struct FwdParams {
-    const float* data;    // [n_ci][n_cx][ns]  traces, ns-sample stride, 16 B aligned
-    const float* vrms;    // [n_vrow][n_vx][n_t] Vrms of output points
+    const float2* pairs;  // [n_ci][n_cx][ns] (d[t], d[t+1]-d[t]); rows 16 B aligned
+    const float* vrms;    // [n_vrow][n_vx][n_t] Vrms of the output points
     float* image;         // [rows][n_ox][n_t]
     const Job* jobs;
     const int* il_pos;    // [n_ci] inline positions
@@ -56,24 +64,53 @@ struct FwdParams {
     int n_vx;             // crosslines of a Vrms plane
     int n_ox;             // output crosslines per row
     int xoff;             // cube / Vrms crossline of output x is x + xoff
+    int max_inl;          // largest i1 - i0 over the jobs (inline-table capacity)
+    int stage_cap;        // samples per ring stage
     float inv_dt, idt2, d_il, d_xl, inv_dxl, tan2, tanth;
-    float ntm1f;  // n_t - 1
-    float ntm1m;  // largest float below n_t - 1
+    float ntm1f;          // n_t - 1
+    float ntm1m;          // largest float below n_t - 1
 };
 
 struct StageMeta {
-    int count;  // traces in this stage, -1 = end of stream
-    float dx2;  // (dx)^2 of the stage's input inline
-    int k[kMaxG];    // cube crossline of each trace
-    int off[kMaxG];  // float offset of the trace window in the stage buffer
-    int ws[kMaxG];   // first sample of the window
-    int lim[kMaxG];  // window length - 2 (largest valid lo - ws)
+    int count;        // traces in this stage, -1 = end of stream
+    int pad[3];
+    int4 m[kMaxG];    // crossline, dx^2 (bits), window base (smem bytes, see consumers),
+                      // window start as float (bits)
+    float shi[kMaxG]; // largest s that stays inside the window
 };
 
 struct TileStats {
-    float vmin, vmax, md2max, t0min, t0max;
+    float vmin, vmax, bmax, t0min, t0max;
     int any;
 };
+
+// Dynamic shared memory layout, shared by the host (sizing) and the kernel.
+struct SmemLayout {
+    unsigned full, empty, meta, stats, inl_klo, inl_pre, inl_dx2, stage, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int max_inl, int cap) {
+    SmemLayout L;
+    unsigned o = 0;
+    L.full = o;
+    o += 8 * kStages;
+    L.empty = o;
+    o += 8 * kStages;
+    L.meta = o = (o + 15) & ~15u;
+    o += sizeof(StageMeta) * kStages;
+    L.stats = o;
+    o += sizeof(TileStats) * kTX;
+    L.inl_klo = o;
+    o += 4 * max_inl;
+    L.inl_pre = o;
+    o += 4 * (max_inl + 1);
+    L.inl_dx2 = o;
+    o += 4 * max_inl;
+    L.stage = o = (o + 127) & ~127u;
+    o += 8u * cap * kStages;
+    L.total = o;
+    return L;
+}
 
 // ----------------------------------------------------------------------------- PTX helpers
 
@@ -128,13 +165,50 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
 
 // TMA bulk copy global -> shared, completion counted on an mbarrier (bytes % 16 == 0,
 // both addresses 16 B aligned).
-__device__ __forceinline__ void tma_load_1d(void* dst_smem, const void* src, uint32_t bytes,
+__device__ __forceinline__ void tma_load_1d(uint32_t dst_smem, const void* src, uint32_t bytes,
                                             uint64_t* bar) {
     asm volatile(
         "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_u32(dst_smem)),
+            "r"(dst_smem),
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
+}
+
+// packed FP32 pairs (sm_100 f32x2 arithmetic)
+__device__ __forceinline__ unsigned long long pk(float2 v) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+    return r;
+}
+__device__ __forceinline__ float2 upk(unsigned long long r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)), "l"(pk(c)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 add2_rm(float2 a, float2 b) {  // rounding toward -inf
+    unsigned long long r;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
 }
 
 __device__ __forceinline__ float warp_max(float v) {
@@ -152,30 +226,29 @@ __device__ __forceinline__ float warp_min(float v) {
 
 // Per output sample constants in the reference's FP32 order (migration_kernel.cpp:115-144).
 // Division and products are pinned to round-to-nearest so the masks see the same numbers
-// as the reference build.
+// as the reference build; that build (GCC, -ffp-contract=fast) fuses v*v + 1e-10.
 struct PointConst {
     bool valid;
     float t0sq, f4, md2, vsq;
 };
 
-// The reference's build (GCC, -ffp-contract=fast) fuses v*v + 1e-10 into one fma.
 __device__ __forceinline__ PointConst point_const(float v, float t0v, float tan2) {
     PointConst p;
-    p.valid = (v >= 1e-5f) && (t0v >= 1e-5f);                       // :121
-    p.t0sq = __fmul_rn(t0v, t0v);                                    // :125
-    p.vsq = __fmul_rn(v, v);                                         // :127
-    float inv_vsq = __fdiv_rn(1.0f, __fmaf_rn(v, v, 1e-10f));        // :128
-    p.f4 = __fmul_rn(4.0f, inv_vsq);                                 // :129
-    float vth = __fmul_rn(__fmul_rn(v, t0v), 0.5f);                  // :133
-    p.md2 = __fmul_rn(__fmul_rn(vth, vth), tan2);                    // :134
+    p.valid = (v >= 1e-5f) && (t0v >= 1e-5f);                 // :121
+    p.t0sq = __fmul_rn(t0v, t0v);                              // :125
+    p.vsq = __fmul_rn(v, v);                                   // :127
+    float inv_vsq = __fdiv_rn(1.0f, __fmaf_rn(v, v, 1e-10f));  // :128
+    p.f4 = __fmul_rn(4.0f, inv_vsq);                           // :129
+    float vth = __fmul_rn(__fmul_rn(v, t0v), 0.5f);            // :133
+    p.md2 = __fmul_rn(__fmul_rn(vth, vth), tan2);              // :134
     return p;
 }
 
 // The reference keeps a term when floor(s) < n_t - 1 with s = fl(sqrt(fma(f4, r2, t0^2)) *
 // inv_dt) in IEEE FP32 (migration_kernel.cpp:209-226, :291-298).  s grows monotonically
-// with r2, so the kept r2 form a prefix [0, R].  Return B = min(md2, R): a term passes both
-// of the reference's masks exactly when r2 <= B (B < 0: no term passes).  Found by bisection
-// on the bit patterns of the non-negative floats in [0, md2] with the reference arithmetic.
+// with r2, so the kept r2 form a prefix [0, R].  pass_bound returns B = min(md2, R): a term
+// passes both of the reference's masks exactly when r2 <= B (B < 0: no term passes).  Found
+// by bisection on the bit patterns of the non-negative floats in [0, md2].
 __device__ __forceinline__ bool range_ok(float r2, float f4, float t0sq, float inv_dt,
                                          float ntm1f) {
     return __fmul_rn(__fsqrt_rn(__fmaf_rn(f4, r2, t0sq)), inv_dt) < ntm1f;
@@ -209,61 +282,108 @@ __device__ __forceinline__ float trace_r2(int dk, float d_xl, float dx2) {
     return __fmaf_rn(dy, dy, dx2);
 }
 
-// ----------------------------------------------------------------------------- forward
+// ----------------------------------------------------------------------------- pair cube
 
-// Producer: derive the window of trace (i, kc) for the tile; size 0 = no terms.
-__device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats& S, int xa,
-                                             int xb, float dx2, int kc, int* ws_out,
-                                             int* size_out) {
-    *ws_out = 0;
-    *size_out = 0;
-    int dkmin = kc < xa ? xa - kc : (kc > xb ? kc - xb : 0);
-    int dkmax = max(abs(kc - xa), abs(kc - xb));
-    float dymin = static_cast<float>(dkmin) * P.d_xl;
-    float dymax = static_cast<float>(dkmax) * P.d_xl;
-    float rmin2 = fmaf(dymin, dymin, dx2);
-    float rmax2 = fmaf(dymax, dymax, dx2);
-    if (rmin2 > S.md2max * 1.0001f + 1e-6f) return;
-    // Unmasked terms need r <= v t0 tan / 2, so t0 >= 2 r_min / (v_max tan).
-    float t0lo = S.t0min;
-    if (P.tanth > 0.0f) t0lo = fmaxf(t0lo, 2.0f * sqrtf(rmin2) / (S.vmax * P.tanth));
-    float tlo = sqrtf(fmaf(t0lo, t0lo, 4.0f * rmin2 / fmaf(S.vmax, S.vmax, 1e-10f)));
-    // and t^2 = t0^2 + f4 r^2 <= t0^2 (1 + tan^2) inside the aperture.
-    float thi2 = fminf(fmaf(S.t0max, S.t0max, 4.0f * rmax2 / fmaf(S.vmin, S.vmin, 1e-10f)),
-                       S.t0max * S.t0max * (1.0f + P.tan2) * 1.0001f);
-    float slo = tlo * P.inv_dt;
-    float shi = fminf(sqrtf(thi2) * P.inv_dt, 1.0e9f);
-    int lolo = max(static_cast<int>(floorf(slo)) - 2, 0);
-    int lohi = min(static_cast<int>(floorf(shi)) + 2, P.n_t - 2);
-    if (lolo > lohi) return;
-    int ws = lolo & ~3;
-    int we = (lohi + 2 + 3) & ~3;  // samples up to lohi + 1, rounded to 16 B
-    *ws_out = ws;
-    *size_out = we - ws;
+// pairs[t] = (d[t], d[t+1] - d[t]) over rows of ns samples (d beyond the row is 0).
+__global__ void pair_kernel(const float* __restrict__ src, float2* __restrict__ dst,
+                            size_t n_rows, int ns) {
+    const size_t n = n_rows * static_cast<size_t>(ns);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int t = static_cast<int>(i % ns);
+        const float a = src[i];
+        const float b = (t + 1 < ns) ? src[i + 1] : 0.0f;
+        dst[i] = make_float2(a, __fsub_rn(b, a));
+    }
 }
 
-template <int J, bool AMP>
-__global__ void __launch_bounds__(32 * (kTX + 1))
-    fwd_kernel(const FwdParams P) {
-    constexpr int TT = 32 * J;
+// ----------------------------------------------------------------------------- forward
+
+// Producer: the window of trace (dx2, kc) for the tile.  size 0: the trace has no term that
+// passes the masks.  ws is even and size even (16-byte TMA granularity for 8-byte samples).
+// Bounds: t >= t0 and, inside the aperture r <= v t0 tan/2, t0 >= 2 r_min / (v_max tan);
+// t^2 = t0^2 + f4 r^2 <= min(t0max^2 + 4 r_max^2 / v_min^2, t0max^2 (1 + tan^2)).
+__device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats& S, int xa,
+                                             int xb, float dx2, int kc, int* ws_out,
+                                             int* size_out, float* shi_out) {
+    *ws_out = 0;
+    *size_out = 0;
+    *shi_out = 0.0f;
+    const int dkmin = kc < xa ? xa - kc : (kc > xb ? kc - xb : 0);
+    const int dkmax = max(abs(kc - xa), abs(kc - xb));
+    const float dymin = static_cast<float>(dkmin) * P.d_xl;
+    const float dymax = static_cast<float>(dkmax) * P.d_xl;
+    const float rmin2 = fmaf(dymin, dymin, dx2);
+    const float rmax2 = fmaf(dymax, dymax, dx2);
+    if (rmin2 > S.bmax * 1.0001f + 1e-6f) return;
+    float t0lo = S.t0min;
+    if (P.tanth > 0.0f) t0lo = fmaxf(t0lo, 2.0f * sqrtf(rmin2) / (S.vmax * P.tanth));
+    const float tlo = sqrtf(fmaf(t0lo, t0lo, 4.0f * rmin2 / fmaf(S.vmax, S.vmax, 1e-10f)));
+    const float thi2 =
+        fminf(fmaf(S.t0max, S.t0max, 4.0f * rmax2 / fmaf(S.vmin, S.vmin, 1e-10f)),
+              S.t0max * S.t0max * (1.0f + P.tan2) * 1.0001f);
+    const float slo = tlo * P.inv_dt;
+    const float shi = fminf(sqrtf(thi2) * P.inv_dt, 1.0e9f);
+    const int lolo = max(static_cast<int>(floorf(slo)) - 2, 0);
+    const int lohi = min(static_cast<int>(floorf(shi)) + 2, P.n_t - 2);
+    if (lolo > lohi) return;
+    const int ws = lolo & ~1;
+    const int we = (lohi + 2) & ~1;  // pairs [ws, we) cover lo in [lolo, lohi]
+    *ws_out = ws;
+    *size_out = we - ws;
+    *shi_out = fminf(P.ntm1m, __uint_as_float(__float_as_uint(static_cast<float>(we)) - 1u));
+}
+
+// One pair of blocks (j, j+1) = (2 pr, 2 pr + 1) for one staged trace.
+// Sample n of the staged window sits at byte sbase + base2 + (bits(2^23 + n) << 3), with
+// 32-bit wrap-around (see the producer).
+template <bool AMP, bool MASK>
+__device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, uint32_t base2,
+                                          float wsf, float shi, const float2& T2,
+                                          const float2& F4, const float2& BB, float2& ACC) {
+    const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
+    const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
+    float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
+    s.x = fminf(fmaxf(s.x, wsf), shi);                       // inside the staged window
+    s.y = fminf(fmaxf(s.y, wsf), shi);
+    const float2 M = make_float2(8388608.0f, 8388608.0f);
+    const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
+    const float2 fr = sub2(s, sub2(mm, M));                  // frac
+    const float2 p0 =
+        *reinterpret_cast<const float2*>(sbase + (base2 + (__float_as_uint(mm.x) << 3)));
+    const float2 p1 =
+        *reinterpret_cast<const float2*>(sbase + (base2 + (__float_as_uint(mm.y) << 3)));
+    float v0 = fmaf(fr.x, p0.y, p0.x);                       // simdInterpolate
+    float v1 = fmaf(fr.y, p1.y, p1.x);
+    if (MASK) {
+        v0 = r2 <= BB.x ? v0 : 0.0f;
+        v1 = r2 <= BB.y ? v1 : 0.0f;
+    }
+    if (AMP)
+        ACC = fma2(make_float2(v0, v1), make_float2(q0, q1), ACC);
+    else
+        ACC = add2(ACC, make_float2(v0, v1));
+}
+
+template <bool AMP>
+__global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
-    uint64_t* empty = full + kStages;
-    StageMeta* meta = reinterpret_cast<StageMeta*>(empty + kStages);
-    TileStats* wstats = reinterpret_cast<TileStats*>(meta + kStages);
-    float* sbuf = reinterpret_cast<float*>(
-        smem_raw + ((sizeof(uint64_t) * 2 * kStages + sizeof(StageMeta) * kStages +
-                     sizeof(TileStats) * kTX + 127) &
-                    ~size_t(127)));
+    const SmemLayout L = smem_layout(P.max_inl, P.stage_cap);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + L.full);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem_raw + L.empty);
+    StageMeta* meta = reinterpret_cast<StageMeta*>(smem_raw + L.meta);
+    TileStats* wstats = reinterpret_cast<TileStats*>(smem_raw + L.stats);
+    const uint32_t stage0 = smem_u32(smem_raw + L.stage);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const Job job = P.jobs[blockIdx.z];
     const int x0 = blockIdx.x * kTX;
-    const int T0 = blockIdx.y * TT;
+    const int T0 = blockIdx.y * kTT;
 
-    // ---- consumers: per-sample constants and tile statistics
-    float t02s[J], f4s[J], md2s[J], acc[J], blkmax[J];
+    // ---- consumers: per-sample constants (4 register pairs) and tile statistics
+    float2 T2[kJ / 2], F4[kJ / 2], BB[kJ / 2], ACC[kJ / 2];
+    float gmax[2], gmin[2];
     float warpmax = -1.0f;
     const int x = x0 + warp - 1;
     const int xv = x + P.xoff;
@@ -271,48 +391,62 @@ __global__ void __launch_bounds__(32 * (kTX + 1))
         const bool xvalid = x < P.n_ox && xv >= 0 && xv < P.n_vx;
         const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
                                     (xvalid ? xv : 0)) * P.n_t;
-        float vmin = 3.0e38f, vmax = 0.0f, md2max = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
+        float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
+        float bj[kJ];
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
+        for (int j = 0; j < kJ; ++j) {
             const int t = T0 + 32 * j + lane;
             float v = 0.0f, t0v = 0.0f;
             if (xvalid && t < P.n_t) {
                 v = __ldg(vp + t);
                 t0v = __ldg(P.t0 + t);
             }
-            PointConst pc = point_const(v, t0v, P.tan2);
-            const float bnd = pass_bound(pc, P.inv_dt, P.ntm1f);
-            acc[j] = 0.0f;
-            if (bnd >= 0.0f) {
-                t02s[j] = pc.t0sq * P.idt2;
-                f4s[j] = pc.f4 * P.idt2;
-                md2s[j] = bnd;
+            const PointConst pc = point_const(v, t0v, P.tan2);
+            const float b = pass_bound(pc, P.inv_dt, P.ntm1f);
+            float t2 = 1.0f, f4 = 0.0f;
+            if (b >= 0.0f) {
+                t2 = pc.t0sq * P.idt2;
+                f4 = pc.f4 * P.idt2;
                 vmin = fminf(vmin, v);
                 vmax = fmaxf(vmax, v);
-                md2max = fmaxf(md2max, bnd);
+                bmax = fmaxf(bmax, b);
                 t0min = fminf(t0min, t0v);
                 t0max = fmaxf(t0max, t0v);
-            } else {
-                t02s[j] = 1.0f;
-                f4s[j] = 0.0f;
-                md2s[j] = -1.0f;
             }
-            blkmax[j] = warp_max(md2s[j]);
-            warpmax = fmaxf(warpmax, blkmax[j]);
+            bj[j] = b;
+            if (j & 1) {
+                T2[j >> 1].y = t2;
+                F4[j >> 1].y = f4;
+                BB[j >> 1].y = b;
+            } else {
+                T2[j >> 1].x = t2;
+                F4[j >> 1].x = f4;
+                BB[j >> 1].x = b;
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < kJ / 2; ++p) ACC[p] = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+            float mx = fmaxf(fmaxf(bj[4 * g], bj[4 * g + 1]), fmaxf(bj[4 * g + 2], bj[4 * g + 3]));
+            float mn = fminf(fminf(bj[4 * g], bj[4 * g + 1]), fminf(bj[4 * g + 2], bj[4 * g + 3]));
+            gmax[g] = warp_max(mx);
+            gmin[g] = warp_min(mn);
+            warpmax = fmaxf(warpmax, gmax[g]);
         }
         vmin = warp_min(vmin);
         vmax = warp_max(vmax);
-        md2max = warp_max(md2max);
+        bmax = warp_max(bmax);
         t0min = warp_min(t0min);
         t0max = warp_max(t0max);
         if (lane == 0) {
             TileStats s;
             s.vmin = vmin;
             s.vmax = vmax;
-            s.md2max = md2max;
+            s.bmax = bmax;
             s.t0min = t0min;
             s.t0max = t0max;
-            s.any = md2max >= 0.0f;
+            s.any = bmax >= 0.0f;
             wstats[warp - 1] = s;
         }
     } else if (lane == 0) {
@@ -329,84 +463,126 @@ __global__ void __launch_bounds__(32 * (kTX + 1))
         TileStats S;
         S.vmin = 3.0e38f;
         S.vmax = 0.0f;
-        S.md2max = -1.0f;
+        S.bmax = -1.0f;
         S.t0min = 3.0e38f;
         S.t0max = 0.0f;
         S.any = 0;
         for (int w = 0; w < kTX; ++w) {
-            TileStats s = wstats[w];
+            const TileStats s = wstats[w];
             if (!s.any) continue;
             S.any = 1;
             S.vmin = fminf(S.vmin, s.vmin);
             S.vmax = fmaxf(S.vmax, s.vmax);
-            S.md2max = fmaxf(S.md2max, s.md2max);
+            S.bmax = fmaxf(S.bmax, s.bmax);
             S.t0min = fminf(S.t0min, s.t0min);
             S.t0max = fmaxf(S.t0max, s.t0max);
         }
         // cube crossline range of the tile's output points
         const int xa = max(x0 + P.xoff, 0);
         const int xb = min(min(x0 + kTX, P.n_ox) - 1 + P.xoff, P.n_vx - 1);
+        int* inl_klo = reinterpret_cast<int*>(smem_raw + L.inl_klo);
+        int* inl_pre = reinterpret_cast<int*>(smem_raw + L.inl_pre);
+        float* inl_dx2 = reinterpret_cast<float*>(smem_raw + L.inl_dx2);
+        const int n_inl = max(job.i1 - job.i0, 0);
+        int total = 0;
+        if (S.any && xa <= xb) {
+            // inline table: crossline range and running trace count per buffer inline
+            for (int base = 0; base < n_inl; base += 32) {
+                const int n = base + lane;
+                int cnt = 0, klo = 0;
+                float dx2 = 0.0f;
+                if (n < n_inl) {
+                    dx2 = inline_dx2(__ldg(P.il_pos + job.i0 + n), job.pos, P.d_il);
+                    if (dx2 <= S.bmax) {
+                        const int K =
+                            static_cast<int>(sqrtf(fmaxf(S.bmax - dx2, 0.0f)) * P.inv_dxl) + 2;
+                        klo = max(0, xa - K);
+                        cnt = max(0, min(P.n_cx - 1, xb + K) - klo + 1);
+                    }
+                    inl_klo[n] = klo;
+                    inl_dx2[n] = dx2;
+                }
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                if (n < n_inl) inl_pre[n] = total + incl - cnt;
+                total += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) inl_pre[n_inl] = total;
+            __syncwarp();
+        }
         uint32_t it = 0;
         bool alive = true;
-        if (S.any && xa <= xb) {
-            for (int i = job.i0; i < job.i1 && alive; ++i) {
-                const float dx2 = inline_dx2(__ldg(P.il_pos + i), job.pos, P.d_il);
-                if (dx2 > S.md2max) continue;
-                const int K = static_cast<int>(sqrtf(fmaxf(S.md2max - dx2, 0.0f)) * P.inv_dxl) + 2;
-                const int klo = max(0, xa - K);
-                const int khi = min(P.n_cx - 1, xb + K);
-                const float* plane = P.data + static_cast<size_t>(i) * P.n_cx * P.ns;
-                int k = klo;
-                while (k <= khi) {
-                    const int kk = k + lane;
-                    int ws = 0, size = 0;
-                    if (kk <= khi) trace_window(P, S, xa, xb, dx2, kk, &ws, &size);
-                    // inclusive prefix sum of window sizes
-                    int cum = size;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        int n = __shfl_up_sync(0xffffffffu, cum, o);
-                        if (lane >= o) cum += n;
-                    }
-                    const bool take = cum <= kStageCap;
-                    const unsigned takemask = __ballot_sync(0xffffffffu, take);
-                    const int consumed = __popc(takemask);
-                    const unsigned nzmask = __ballot_sync(0xffffffffu, take && size > 0);
-                    const int n = __popc(nzmask);
-                    if (n > 0) {
-                        const int stage = it % kStages;
-                        const uint32_t par = ((it / kStages) & 1u) ^ 1u;
-                        int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
-                        if (!__shfl_sync(0xffffffffu, ok, 0)) {
-                            alive = false;
-                            break;
-                        }
-                        StageMeta& m = meta[stage];
-                        const int total = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
-                        if (take && size > 0) {
-                            const int slot = __popc(nzmask & ((1u << lane) - 1u));
-                            m.k[slot] = kk;
-                            m.off[slot] = cum - size;
-                            m.ws[slot] = ws;
-                            m.lim[slot] = size - 2;
-                        }
-                        if (lane == 0) {
-                            m.count = n;
-                            m.dx2 = dx2;
-                        }
-                        __threadfence_block();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive_expect_tx(&full[stage], total * 4u);
-                        __syncwarp();
-                        if (take && size > 0)
-                            tma_load_1d(sbuf + stage * kStageCap + (cum - size),
-                                        plane + static_cast<size_t>(kk) * P.ns + ws,
-                                        static_cast<uint32_t>(size) * 4u, &full[stage]);
-                        ++it;
-                    }
-                    k += consumed;
+        int f = 0;
+        while (f < total && alive) {
+            const int idx = f + lane;
+            int ws = 0, size = 0, kc = 0, row = 0;
+            float dx2 = 0.0f, shi = 0.0f;
+            if (idx < total) {
+                // buffer inline of flat trace idx: the last n with inl_pre[n] <= idx
+                int lo = 0, hi = n_inl - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (inl_pre[mid] <= idx)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
                 }
+                kc = inl_klo[lo] + (idx - inl_pre[lo]);
+                dx2 = inl_dx2[lo];
+                row = job.i0 + lo;
+                trace_window(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
             }
+            // inclusive prefix sum of window sizes; take the lanes that fit one stage
+            int cum = size;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, cum, o);
+                if (lane >= o) cum += v;
+            }
+            const bool take = cum <= P.stage_cap;
+            const unsigned takemask = __ballot_sync(0xffffffffu, take);
+            const int consumed = __popc(takemask);
+            const unsigned nzmask = __ballot_sync(0xffffffffu, take && size > 0);
+            const int n = __popc(nzmask);
+            if (n > 0) {
+                const int stage = it % kStages;
+                const uint32_t par = ((it / kStages) & 1u) ^ 1u;
+                const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    alive = false;
+                    break;
+                }
+                StageMeta& m = meta[stage];
+                const int tot = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
+                const uint32_t dst_rel =
+                    L.stage + (static_cast<uint32_t>(stage) * P.stage_cap + (cum - size)) * 8u;
+                const uint32_t dst = stage0 + (dst_rel - L.stage);
+                if (take && size > 0) {
+                    const int slot = __popc(nzmask & ((1u << lane) - 1u));
+                    // consumers find sample n of the window at byte
+                    // base2 + (bits(2^23 + n) << 3) from the shared-memory base (32-bit
+                    // wrap-around): base2 = dst_rel - 8 ws - (0x4B000000 << 3)
+                    m.m[slot] = make_int4(kc, __float_as_int(dx2),
+                                          static_cast<int>(dst_rel - 8u * ws - 0x58000000u),
+                                          __float_as_int(static_cast<float>(ws)));
+                    m.shi[slot] = shi;
+                }
+                if (lane == 0) m.count = n;
+                __threadfence_block();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_expect_tx(&full[stage], static_cast<uint32_t>(tot) * 8u);
+                __syncwarp();
+                if (take && size > 0)
+                    tma_load_1d(dst,
+                                P.pairs + (static_cast<size_t>(row) * P.n_cx + kc) * P.ns + ws,
+                                static_cast<uint32_t>(size) * 8u, &full[stage]);
+                ++it;
+            }
+            f += consumed;
         }
         // end-of-stream marker
         if (alive && lane == 0) {
@@ -430,37 +606,27 @@ __global__ void __launch_bounds__(32 * (kTX + 1))
         const StageMeta& m = meta[stage];
         const int cnt = m.count;
         if (cnt < 0) break;
-        const float dx2 = m.dx2;
-        const float* sb = sbuf + stage * kStageCap;
         for (int g = 0; g < cnt; ++g) {
-            const int kc = m.k[g];
-            const float r2 = trace_r2(kc - xv, P.d_xl, dx2);
+            const int4 md = m.m[g];
+            const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
             if (r2 > warpmax) continue;
-            const float* tb = sb + m.off[g];
-            const int ws = m.ws[g];
-            const unsigned lim = static_cast<unsigned>(m.lim[g]);
+            const uint32_t base2 = static_cast<uint32_t>(md.z);
+            const float wsf = __int_as_float(md.w);
+            const float shi = m.shi[g];
 #pragma unroll
-            for (int j = 0; j < J; ++j) {
-                if (r2 > blkmax[j]) continue;
-                if (r2 <= md2s[j]) {  // both reference masks, exactly (pass_bound)
-                    const float t2 = __fmaf_rn(f4s[j], r2, t02s[j]);  // (t / dt)^2
-                    const float q = rsqrtf(t2);                        // dt / t
-                    // t / dt; the reference's s is < n_t - 1 here, keep ours below it too
-                    const float s = fminf(t2 * q, P.ntm1m);
-                    const float mm = __fadd_rd(s, 8388608.0f);
-                    const int lo = __float_as_int(mm) - 0x4B000000;  // floor(s)
-                    const float fr = s - (mm - 8388608.0f);
-#ifdef PSM_DEBUG_BOUNDS
-                    if (static_cast<unsigned>(lo - ws) > lim) atomicOr(P.err, PSM_DEV_ERR_WINDOW);
-#endif
-                    const unsigned idx = min(static_cast<unsigned>(lo - ws), lim);
-                    const float a = tb[idx];
-                    const float b = tb[idx + 1];
-                    const float val = __fmaf_rn(fr, b - a, a);
-                    if (AMP)
-                        acc[j] = __fmaf_rn(val, q, acc[j]);
-                    else
-                        acc[j] += val;
+            for (int gr = 0; gr < 2; ++gr) {
+                if (r2 <= gmax[gr]) {
+                    if (r2 <= gmin[gr]) {  // every lane of both pairs passes
+                        term_pair<AMP, false>(smem_raw, r2, base2, wsf, shi, T2[2 * gr], F4[2 * gr],
+                                              BB[2 * gr], ACC[2 * gr]);
+                        term_pair<AMP, false>(smem_raw, r2, base2, wsf, shi, T2[2 * gr + 1],
+                                              F4[2 * gr + 1], BB[2 * gr + 1], ACC[2 * gr + 1]);
+                    } else {
+                        term_pair<AMP, true>(smem_raw, r2, base2, wsf, shi, T2[2 * gr], F4[2 * gr],
+                                             BB[2 * gr], ACC[2 * gr]);
+                        term_pair<AMP, true>(smem_raw, r2, base2, wsf, shi, T2[2 * gr + 1],
+                                             F4[2 * gr + 1], BB[2 * gr + 1], ACC[2 * gr + 1]);
+                    }
                 }
             }
         }
@@ -476,16 +642,18 @@ __global__ void __launch_bounds__(32 * (kTX + 1))
                                     (xvalid ? xv : 0)) * P.n_t;
         float* op = P.image + (static_cast<size_t>(job.row) * P.n_ox + x) * P.n_t;
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
+        for (int j = 0; j < kJ; ++j) {
             const int t = T0 + 32 * j + lane;
             if (t < P.n_t) {
+                const float b = (j & 1) ? BB[j >> 1].y : BB[j >> 1].x;
+                const float a = (j & 1) ? ACC[j >> 1].y : ACC[j >> 1].x;
                 float o = 0.0f;
-                if (md2s[j] >= 0.0f) {
+                if (b >= 0.0f) {
                     if (AMP) {
                         const float v = __ldg(vp + t);
-                        o = acc[j] * __fdiv_rn(P.inv_dt, __fmul_rn(v, v));
+                        o = a * __fdiv_rn(P.inv_dt, __fmul_rn(v, v));
                     } else {
-                        o = acc[j];
+                        o = a;
                     }
                 }
                 op[t] = o;
