@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--workload", choices=["config2", "config2_201", "config1"],
                    default="config2")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    p.add_argument("--variant", type=int, default=0,
+                   help="forward kernel variant (0: autotune)")
     p.add_argument("--cpu-rows", type=int, default=2,
                    help="output inlines in the bounded CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -273,6 +275,12 @@ def run_ours(args):
     m.set_vrms(W.vrms_cube())
     n_terms = m.count_terms()
     stream = torch.cuda.ExternalStream(m.stream_handle())
+    tuned = None
+    if args.variant:
+        m.set_variant(args.variant)
+    else:  # project autotuner: one timed launch per kernel variant, keep the fastest
+        best, ms_v = m.autotune()
+        tuned = {Migrator.VARIANTS[v]: round(t, 3) for v, t in ms_v.items()}
 
     for _ in range(max(args.warmup, 0)):
         m.forward_async()
@@ -377,7 +385,9 @@ def run_ours(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic (seeded)",
                 "config": config_dict(W, g, {"n_terms": n_terms,
-                                             "parallelism": f"replicas x{world}"}),
+                                             "parallelism": f"replicas x{world}",
+                                             "variant": Migrator.VARIANTS[m.variant()],
+                                             "autotune_ms": tuned}),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": args.steps, "clocks": clocks}
         print(json.dumps(line), flush=True)

@@ -101,6 +101,25 @@ int psm_get_image(psm_ctx *ctx, float *image);
 /* Raw CUDA stream of the ctx (a cudaStream_t). */
 int psm_stream(psm_ctx *ctx, void **stream);
 
+/* Forward-kernel variants: f32x2-packed or scalar FP32 arithmetic for each pair of 32-sample
+ * blocks, and 2 or 4 blocks behind one warp-uniform skip test.  All give the same masks and
+ * the same terms; they differ in instruction count.  PSM_FWD_DEFAULT lets the library pick
+ * (the result of psm_autotune once it has run on the ctx). */
+typedef enum {
+    PSM_FWD_DEFAULT = 0,
+    PSM_FWD_SCALAR_G2 = 1,
+    PSM_FWD_SCALAR_G4 = 2,
+    PSM_FWD_PACKED_G2 = 3,
+    PSM_FWD_PACKED_G4 = 4,
+    PSM_FWD_N_VARIANTS = 5
+} psm_fwd_variant;
+int psm_set_variant(psm_ctx *ctx, int variant);
+int psm_get_variant(psm_ctx *ctx, int *variant);
+/* Time one forward launch of every variant on the resident cube (CUDA events on the ctx
+ * stream), keep the fastest for this ctx.  ms[PSM_FWD_N_VARIANTS] (may be NULL) receives the
+ * times, ms[0] unused; *best (may be NULL) the chosen variant. */
+int psm_autotune(psm_ctx *ctx, float *ms, int *best);
+
 /* Number of (output sample, input trace) terms that pass every mask of the reference
  * (migration_kernel.cpp:166, :207/:286, :226/:298) over the real input traces, counted on
  * the GPU with the forward kernel's own arithmetic. */

@@ -77,26 +77,40 @@ size_t fwd_smem(const FwdParams& P) {
     return b <= kMaxDynSmem ? b : 0;
 }
 
+template <bool AMP, bool PACKED, int GB>
+cudaError_t launch_fwd_v(const FwdParams& P, int n_jobs, size_t smem, cudaStream_t s) {
+    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + psm::kTT - 1) / psm::kTT, n_jobs);
+    dim3 block(32 * (psm::kTX + 1));
+    cudaError_t e = cudaFuncSetAttribute(psm::fwd_kernel<AMP, PACKED, GB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    psm::fwd_kernel<AMP, PACKED, GB><<<grid, block, smem, s>>>(P);
+    return cudaGetLastError();
+}
+
+template <bool AMP>
+cudaError_t launch_fwd_amp(const FwdParams& P, int n_jobs, int variant, size_t smem,
+                           cudaStream_t s) {
+    switch (variant) {
+        case PSM_FWD_SCALAR_G2: return launch_fwd_v<AMP, false, 2>(P, n_jobs, smem, s);
+        case PSM_FWD_SCALAR_G4: return launch_fwd_v<AMP, false, 4>(P, n_jobs, smem, s);
+        case PSM_FWD_PACKED_G2: return launch_fwd_v<AMP, true, 2>(P, n_jobs, smem, s);
+        case PSM_FWD_PACKED_G4: return launch_fwd_v<AMP, true, 4>(P, n_jobs, smem, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+constexpr int kDefaultVariant = PSM_FWD_PACKED_G4;
+
 // Launch the forward kernel for n_jobs jobs (P.max_inl and P.stage_cap set).
-cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, cudaStream_t s) {
+cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, int variant, cudaStream_t s) {
     if (n_jobs <= 0 || P.n_ox <= 0 || P.n_t <= 0) return cudaSuccess;
     const size_t smem = fwd_smem(P);
     if (!smem) return cudaErrorInvalidValue;
-    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + psm::kTT - 1) / psm::kTT, n_jobs);
-    dim3 block(32 * (psm::kTX + 1));
-    cudaError_t e;
-    if (amp) {
-        e = cudaFuncSetAttribute(psm::fwd_kernel<true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        psm::fwd_kernel<true><<<grid, block, smem, s>>>(P);
-    } else {
-        e = cudaFuncSetAttribute(psm::fwd_kernel<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        psm::fwd_kernel<false><<<grid, block, smem, s>>>(P);
-    }
-    return cudaGetLastError();
+    if (variant == PSM_FWD_DEFAULT) variant = kDefaultVariant;
+    return amp ? launch_fwd_amp<true>(P, n_jobs, variant, smem, s)
+               : launch_fwd_amp<false>(P, n_jobs, variant, smem, s);
 }
 
 // pairs[n_rows][ns] from the fp32 rows (pair_kernel).
@@ -131,6 +145,7 @@ struct psm_ctx {
     bool have_geom = false, have_traces = false, have_vrms = false;
     psm_geom g{};
     int ns = 0;
+    int variant = PSM_FWD_DEFAULT;
     std::vector<Job> jobs;       // one per distinct migrated inline
     std::vector<Job> jobs_all;   // one per output row (term counting)
     std::vector<std::pair<int, int>> copies;  // (dst row, src row) duplicated output rows
@@ -341,7 +356,7 @@ int psm_forward_async(psm_ctx* c) {
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
     FwdParams P = volume_params(c);
     PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
-                                   c->g.amp_correction != 0, c->stream));
+                                   c->g.amp_correction != 0, c->variant, c->stream));
     // padded output inlines repeat the migrated edge inline (main.cpp:268-285)
     const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
     for (const auto& cp : c->copies)
@@ -350,6 +365,51 @@ int psm_forward_async(psm_ctx* c) {
                                             row * sizeof(float), cudaMemcpyDeviceToDevice,
                                             c->stream));
     return PSM_OK;
+}
+
+int psm_set_variant(psm_ctx* c, int variant) {
+    if (!c || variant < 0 || variant >= PSM_FWD_N_VARIANTS) return PSM_ERR_ARG;
+    c->variant = variant;
+    return PSM_OK;
+}
+
+int psm_get_variant(psm_ctx* c, int* variant) {
+    if (!c || !variant) return PSM_ERR_ARG;
+    *variant = c->variant == PSM_FWD_DEFAULT ? kDefaultVariant : c->variant;
+    return PSM_OK;
+}
+
+int psm_autotune(psm_ctx* c, float* ms, int* best) {
+    if (!c) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_traces || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry, traces and vrms must be set");
+    cudaSetDevice(c->device);
+    cudaEvent_t e0, e1;
+    PSM_CUDA_TRY(c->st, cudaEventCreate(&e0));
+    PSM_CUDA_TRY(c->st, cudaEventCreate(&e1));
+    int pick = kDefaultVariant;
+    float pick_ms = 3.0e38f;
+    int rc = PSM_OK;
+    for (int v = 1; v < PSM_FWD_N_VARIANTS && rc == PSM_OK; ++v) {
+        c->variant = v;
+        float t = 0.0f;
+        if ((rc = psm_forward_async(c)) != PSM_OK) break;  // warm (first launch, attribute)
+        cudaEventRecord(e0, c->stream);
+        if ((rc = psm_forward_async(c)) != PSM_OK) break;
+        cudaEventRecord(e1, c->stream);
+        if ((rc = psm_synchronize(c)) != PSM_OK) break;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (ms) ms[v] = t;
+        if (t < pick_ms) {
+            pick_ms = t;
+            pick = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->variant = pick;
+    if (rc == PSM_OK && best) *best = pick;
+    return rc;
 }
 
 int psm_synchronize(psm_ctx* c) {
@@ -531,7 +591,7 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
     P.max_inl = std::max<int>(static_cast<int>(n_buf_il), 1);
     P.stage_cap = stage_cap(ns);
     fill_consts(P, dt, inline_bin_size, crossline_bin_size, tan_theta_sq);
-    PSM_INL_TRY(launch_fwd(P, 1, amp_correction != 0, s));
+    PSM_INL_TRY(launch_fwd(P, 1, amp_correction != 0, PSM_FWD_DEFAULT, s));
     PSM_INL_TRY(cudaMemcpyAsync(output_slice, S->out.p, n_out_xl * n_t * sizeof(float),
                                 cudaMemcpyDeviceToHost, s));
     int h = 0;

@@ -337,10 +337,35 @@ __device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats
 // One pair of blocks (j, j+1) = (2 pr, 2 pr + 1) for one staged trace.
 // Sample n of the staged window sits at byte sbase + base2 + (bits(2^23 + n) << 3), with
 // 32-bit wrap-around (see the producer).
+// One term of block-pair component (scalar FP32 arithmetic).
 template <bool AMP, bool MASK>
+__device__ __forceinline__ void term_one(const unsigned char* sbase, float r2, uint32_t base2,
+                                         float wsf, float shi, float T2, float F4, float BB,
+                                         float& ACC) {
+    const float t2 = __fmaf_rn(F4, r2, T2);                  // (t / dt)^2
+    const float q = rsqrtf(t2);                              // dt / t
+    const float s = fminf(fmaxf(t2 * q, wsf), shi);          // t / dt inside the window
+    const float mm = __fadd_rd(s, 8388608.0f);               // 2^23 + floor(s)
+    const float fr = s - (mm - 8388608.0f);                  // frac
+    const float2 p =
+        *reinterpret_cast<const float2*>(sbase + (base2 + (__float_as_uint(mm) << 3)));
+    float v = __fmaf_rn(fr, p.y, p.x);                       // simdInterpolate
+    if (MASK) v = r2 <= BB ? v : 0.0f;
+    if (AMP)
+        ACC = __fmaf_rn(v, q, ACC);
+    else
+        ACC += v;
+}
+
+template <bool AMP, bool MASK, bool PACKED>
 __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, uint32_t base2,
                                           float wsf, float shi, const float2& T2,
                                           const float2& F4, const float2& BB, float2& ACC) {
+    if (!PACKED) {
+        term_one<AMP, MASK>(sbase, r2, base2, wsf, shi, T2.x, F4.x, BB.x, ACC.x);
+        term_one<AMP, MASK>(sbase, r2, base2, wsf, shi, T2.y, F4.y, BB.y, ACC.y);
+        return;
+    }
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
     const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
     float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
@@ -365,8 +390,13 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
         ACC = add2(ACC, make_float2(v0, v1));
 }
 
-template <bool AMP>
+// Kernel variants: PACKED selects f32x2 or scalar FP32 arithmetic for a block pair; GB is
+// the number of 32-sample blocks behind one warp-uniform skip test (2 or 4).
+template <bool AMP, bool PACKED, int GB>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
+    static_assert(GB == 2 || GB == 4, "skip groups of 2 or 4 blocks");
+    constexpr int NG = kJ / GB;  // skip groups per lane
+    constexpr int PG = GB / 2;   // block pairs per group
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + L.full);
@@ -383,7 +413,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
 
     // ---- consumers: per-sample constants (4 register pairs) and tile statistics
     float2 T2[kJ / 2], F4[kJ / 2], BB[kJ / 2], ACC[kJ / 2];
-    float gmax[2], gmin[2];
+    float gmax[NG], gmin[NG];
     float warpmax = -1.0f;
     const int x = x0 + warp - 1;
     const int xv = x + P.xoff;
@@ -427,9 +457,13 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
 #pragma unroll
         for (int p = 0; p < kJ / 2; ++p) ACC[p] = make_float2(0.0f, 0.0f);
 #pragma unroll
-        for (int g = 0; g < 2; ++g) {
-            float mx = fmaxf(fmaxf(bj[4 * g], bj[4 * g + 1]), fmaxf(bj[4 * g + 2], bj[4 * g + 3]));
-            float mn = fminf(fminf(bj[4 * g], bj[4 * g + 1]), fminf(bj[4 * g + 2], bj[4 * g + 3]));
+        for (int g = 0; g < NG; ++g) {
+            float mx = bj[GB * g], mn = bj[GB * g];
+#pragma unroll
+            for (int b = 1; b < GB; ++b) {
+                mx = fmaxf(mx, bj[GB * g + b]);
+                mn = fminf(mn, bj[GB * g + b]);
+            }
             gmax[g] = warp_max(mx);
             gmin[g] = warp_min(mn);
             warpmax = fmaxf(warpmax, gmax[g]);
@@ -614,18 +648,18 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
             const float wsf = __int_as_float(md.w);
             const float shi = m.shi[g];
 #pragma unroll
-            for (int gr = 0; gr < 2; ++gr) {
+            for (int gr = 0; gr < NG; ++gr) {
                 if (r2 <= gmax[gr]) {
-                    if (r2 <= gmin[gr]) {  // every lane of both pairs passes
-                        term_pair<AMP, false>(smem_raw, r2, base2, wsf, shi, T2[2 * gr], F4[2 * gr],
-                                              BB[2 * gr], ACC[2 * gr]);
-                        term_pair<AMP, false>(smem_raw, r2, base2, wsf, shi, T2[2 * gr + 1],
-                                              F4[2 * gr + 1], BB[2 * gr + 1], ACC[2 * gr + 1]);
+                    if (r2 <= gmin[gr]) {  // every lane of the group passes
+#pragma unroll
+                        for (int p = PG * gr; p < PG * (gr + 1); ++p)
+                            term_pair<AMP, false, PACKED>(smem_raw, r2, base2, wsf, shi, T2[p],
+                                                          F4[p], BB[p], ACC[p]);
                     } else {
-                        term_pair<AMP, true>(smem_raw, r2, base2, wsf, shi, T2[2 * gr], F4[2 * gr],
-                                             BB[2 * gr], ACC[2 * gr]);
-                        term_pair<AMP, true>(smem_raw, r2, base2, wsf, shi, T2[2 * gr + 1],
-                                             F4[2 * gr + 1], BB[2 * gr + 1], ACC[2 * gr + 1]);
+#pragma unroll
+                        for (int p = PG * gr; p < PG * (gr + 1); ++p)
+                            term_pair<AMP, true, PACKED>(smem_raw, r2, base2, wsf, shi, T2[p],
+                                                         F4[p], BB[p], ACC[p]);
                     }
                 }
             }

@@ -247,6 +247,24 @@ class Migrator:
         check(self._L.psm_count_terms(self._ctx, ctypes.byref(n)), self._err)
         return int(n.value)
 
+    VARIANTS = {1: "scalar/g2", 2: "scalar/g4", 3: "packed/g2", 4: "packed/g4"}
+
+    def set_variant(self, variant: int) -> None:
+        check(self._L.psm_set_variant(self._ctx, int(variant)), self._err)
+
+    def variant(self) -> int:
+        v = ctypes.c_int()
+        check(self._L.psm_get_variant(self._ctx, ctypes.byref(v)), self._err)
+        return v.value
+
+    def autotune(self):
+        """Time every forward variant once on the resident cube and keep the fastest.
+        Returns (best variant, {variant: ms})."""
+        ms = np.zeros(5, dtype=np.float32)
+        best = ctypes.c_int()
+        check(self._L.psm_autotune(self._ctx, ms.ctypes.data, ctypes.byref(best)), self._err)
+        return best.value, {v: float(ms[v]) for v in self.VARIANTS}
+
     def count_terms_rows(self) -> np.ndarray:
         out = np.zeros(self.geom.n_oi, dtype=np.int64)
         check(self._L.psm_count_terms_rows(self._ctx, out.ctypes.data), self._err)

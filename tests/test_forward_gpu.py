@@ -85,6 +85,30 @@ def test_inline_dropin_matches_oracle():
         assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (cur_il, xs, rms, mx)
 
 
+def test_variants_are_bit_identical_and_autotune_picks_one():
+    """Packed (f32x2) and scalar arithmetic perform the same IEEE operations per term, and
+    masked terms add exact zeros, so every variant gives the same image bit for bit."""
+    W = S.random_workload(31, 14, 17, 400, vel_kind="lateral", angle=50.0, pad_xl=2)
+    g = geometry_for(W)
+    with Migrator(0) as m:
+        m.set_geometry(g)
+        m.set_traces(W.data)
+        m.set_vrms(W.vrms_cube())
+        imgs = {}
+        for v in Migrator.VARIANTS:
+            m.set_variant(v)
+            assert m.variant() == v
+            imgs[v] = m.forward()
+        best, ms = m.autotune()
+        assert best in Migrator.VARIANTS and all(t > 0 for t in ms.values())
+        assert m.variant() == best
+        after = m.forward()
+    ref = imgs[1]
+    for v, img in imgs.items():
+        assert np.array_equal(img, ref), v
+    assert np.array_equal(after, ref)
+
+
 def test_forward_is_linear_and_repeatable():
     W = S.random_workload(21, 10, 12, 200, vel_kind="lateral", angle=50.0)
     g = geometry_for(W)
