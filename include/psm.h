@@ -143,6 +143,27 @@ int psm_kirchhoff_inline(const float *input_buffer, size_t n_buf_il, size_t n_bu
 /* Message of the last psm_kirchhoff_inline failure on this thread. */
 const char *psm_kirchhoff_inline_error(void);
 
+/* Forward migration that allocates no device memory (this entry point has no counterpart in
+ * the reference).  It is for callers that must not call cudaMalloc: applications whose device
+ * memory is owned by their own pool or framework allocator, and pipelines that set up all
+ * memory once and cannot afford the implicit device synchronisation of cudaMalloc/cudaFree.
+ * The caller owns every input and output; all are device pointers:
+ *   d_pairs   [n_il][n_xl][ns] pairs of floats (d[t], d[t+1] - d[t]), ns = (n_t + 7) & ~7,
+ *             d beyond n_t - 1 taken as 0; 16-byte aligned
+ *   d_vrms    [n_il][n_xl][n_t] Vrms of the output points
+ *   d_image   [n_oi][n_ox][n_t] output, fully overwritten
+ * g and out_center (host, [n_oi] or NULL) mean what they mean for psm_set_geometry; stream is
+ * a cudaStream_t (NULL: the default stream).  The call returns when the image is complete.
+ * Its only working memory is one file-scope device array of PSM_NOALLOC_SCRATCH_BYTES
+ * (192 KiB), which every GPU that loads the library holds until the process exits; it limits
+ * n_oi <= 4096, n_il <= 4096 and n_t <= 16384 (PSM_ERR_UNSUPPORTED beyond).  The first call on
+ * a device looks up that array's device address, so make it before any stream capture.  All
+ * calls share the array and it keeps the last call's contents: calls that overlap on the GPU
+ * race, so serialise them. */
+#define PSM_NOALLOC_SCRATCH_BYTES (192 * 1024)
+int psm_forward_noalloc(const psm_geom *g, const int32_t *out_center, const float *d_pairs,
+                        const float *d_vrms, float *d_image, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -605,3 +606,135 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
 const char* psm_kirchhoff_inline_error(void) { return tl_inline_error.c_str(); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------- no allocation
+//
+// psm_forward_noalloc runs the forward kernel on caller-owned device buffers.  Its working
+// memory (error word, job table, inline positions, time axis) lives in this one file-scope
+// device array instead of cudaMalloc'd buffers.  On the host, g_noalloc_scratch names a
+// host-side stand-in, not device memory: kernels only ever receive the address that
+// cudaGetSymbolAddress returns for the current device.
+
+namespace {
+
+constexpr int kNoallocMaxRows = 4096;    // output inlines
+constexpr int kNoallocMaxInl = 4096;     // input inlines
+constexpr int kNoallocMaxT = 16384;      // samples per trace
+constexpr size_t kNoallocErr = 0;        // int
+constexpr size_t kNoallocJobs = 256;     // Job[kNoallocMaxRows]
+constexpr size_t kNoallocPos = kNoallocJobs + ((sizeof(Job) * kNoallocMaxRows + 255) & ~size_t(255));
+constexpr size_t kNoallocT0 = kNoallocPos + sizeof(int) * kNoallocMaxInl;
+static_assert(kNoallocT0 + sizeof(float) * kNoallocMaxT <= PSM_NOALLOC_SCRATCH_BYTES,
+              "no-allocation scratch layout exceeds its array");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[PSM_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up once per device).
+cudaError_t noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int psm_forward_noalloc(const psm_geom* g, const int32_t* out_center,
+                                   const float* d_pairs, const float* d_vrms, float* d_image,
+                                   void* stream) {
+    if (!g || !d_pairs || !d_vrms || !d_image) return PSM_ERR_ARG;
+    if (g->n_il <= 0 || g->n_xl <= 0 || g->n_t <= 0 || g->n_oi <= 0 || g->n_ox <= 0 ||
+        g->pad_il < 0 || g->pad_xl < 0 || g->m_il < 0 || !(g->dt > 0.0f) ||
+        !(g->d_il > 0.0f) || !(g->d_xl > 0.0f) || !(g->tan2_theta >= 0.0f) ||
+        g->precision != PSM_F32 || (reinterpret_cast<uintptr_t>(d_pairs) & 15u))
+        return PSM_ERR_ARG;
+    if (g->n_oi > kNoallocMaxRows || g->n_il > kNoallocMaxInl || g->n_t > kNoallocMaxT)
+        return PSM_ERR_UNSUPPORTED;
+    const int ns = trace_stride(g->n_t);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    // jobs: one per distinct migrated inline, and the output rows that repeat it
+    // (main.cpp:258-288, migration_kernel.cpp:404-409); fixed-size host arrays, no heap
+    Job jobs[kNoallocMaxRows];
+    int16_t first_row_of[kNoallocMaxInl];
+    int16_t dup_dst[kNoallocMaxRows], dup_src[kNoallocMaxRows];
+    int n_jobs = 0, n_dup = 0, max_inl = 1;
+    for (int i = 0; i < g->n_il; ++i) first_row_of[i] = -1;
+    for (int o = 0; o < g->n_oi; ++o) {
+        const int cc = out_center ? out_center[o]
+                                  : std::min(std::max(o - g->pad_il, 0), g->n_il - 1);
+        if (cc < 0 || cc >= g->n_il) return PSM_ERR_ARG;
+        const int rs = std::max(0, cc - g->m_il), re = std::min(g->n_il, cc + g->m_il + 1);
+        Job j{o, cc, cc, std::max(0, rs - g->pad_il), std::min(g->n_il, re + g->pad_il)};
+        max_inl = std::max(max_inl, j.i1 - j.i0);
+        if (first_row_of[cc] < 0) {
+            first_row_of[cc] = static_cast<int16_t>(o);
+            jobs[n_jobs++] = j;
+        } else {
+            dup_dst[n_dup] = static_cast<int16_t>(o);
+            dup_src[n_dup++] = first_row_of[cc];
+        }
+    }
+    FwdParams P{};
+    P.n_ci = g->n_il;
+    P.n_cx = g->n_xl;
+    P.n_t = g->n_t;
+    P.ns = ns;
+    P.n_vx = g->n_xl;
+    P.n_ox = g->n_ox;
+    P.xoff = -g->pad_xl;
+    P.max_inl = max_inl;
+    P.stage_cap = stage_cap(ns);
+    if (!fwd_smem(P)) return PSM_ERR_UNSUPPORTED;
+    fill_consts(P, g->dt, g->d_il, g->d_xl, g->tan2_theta);
+
+    unsigned char* scratch = nullptr;
+    if (noalloc_scratch(&scratch) != cudaSuccess) return PSM_ERR_CUDA;
+    int pos[kNoallocMaxInl];
+    float t0[kNoallocMaxT];
+    for (int i = 0; i < g->n_il; ++i) pos[i] = i;
+    for (int i = 0; i < g->n_t; ++i)
+        t0[i] = static_cast<float>(static_cast<double>(i) * g->dt_seconds);  // main.cpp:216
+#define PSM_NA_TRY(call)                                                            \
+    do {                                                                            \
+        if ((call) != cudaSuccess) return PSM_ERR_CUDA;                             \
+    } while (0)
+    // the array keeps the last call's contents: reset the error word, rewrite the tables
+    PSM_NA_TRY(cudaMemsetAsync(scratch + kNoallocErr, 0, sizeof(int), s));
+    PSM_NA_TRY(cudaMemcpyAsync(scratch + kNoallocJobs, jobs, sizeof(Job) * n_jobs,
+                               cudaMemcpyHostToDevice, s));
+    PSM_NA_TRY(cudaMemcpyAsync(scratch + kNoallocPos, pos, sizeof(int) * g->n_il,
+                               cudaMemcpyHostToDevice, s));
+    PSM_NA_TRY(cudaMemcpyAsync(scratch + kNoallocT0, t0, sizeof(float) * g->n_t,
+                               cudaMemcpyHostToDevice, s));
+    P.pairs = reinterpret_cast<const float2*>(d_pairs);
+    P.vrms = d_vrms;
+    P.image = d_image;
+    P.jobs = reinterpret_cast<const Job*>(scratch + kNoallocJobs);
+    P.il_pos = reinterpret_cast<const int*>(scratch + kNoallocPos);
+    P.t0 = reinterpret_cast<const float*>(scratch + kNoallocT0);
+    P.err = reinterpret_cast<int*>(scratch + kNoallocErr);
+    PSM_NA_TRY(launch_fwd(P, n_jobs, g->amp_correction != 0, PSM_FWD_DEFAULT, s));
+    const size_t row = static_cast<size_t>(g->n_ox) * g->n_t;
+    for (int k = 0; k < n_dup; ++k)
+        PSM_NA_TRY(cudaMemcpyAsync(d_image + dup_dst[k] * row, d_image + dup_src[k] * row,
+                                   row * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    int h = 0;
+    PSM_NA_TRY(cudaMemcpyAsync(&h, scratch + kNoallocErr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PSM_NA_TRY(cudaStreamSynchronize(s));
+#undef PSM_NA_TRY
+    return h ? PSM_ERR_DEVICE : PSM_OK;
+}
