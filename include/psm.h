@@ -101,6 +101,20 @@ int psm_get_image(psm_ctx *ctx, float *image);
 /* Raw CUDA stream of the ctx (a cudaStream_t). */
 int psm_stream(psm_ctx *ctx, void **stream);
 
+/* Adjoint of psm_forward (demigration / spray, M^T): data[n_il][n_xl][n_t] (host, output)
+ * from image[n_oi][n_ox][n_t] (host).  Every term of the forward is spread back with its
+ * transposed interpolation weights (1 - frac, frac) and the same amplitude weight, so
+ * <M d, m> = <d, M^T m> to FP32 summation noise.  Needs geometry and vrms; replaces the
+ * resident traces with nothing (they stay). */
+int psm_adjoint(psm_ctx *ctx, const float *image, float *data);
+
+/* Least-squares migration: `iters` iterations of CG (CGLS) on min ||M^T m - data||^2 from
+ * m = 0, with FP32 operators and FP64 inner products and step lengths computed on the GPU.
+ * data [n_il][n_xl][n_t] (host) in, image [n_oi][n_ox][n_t] (host) out, resid[iters + 1]
+ * (host, may be NULL) the data-residual norms ||M^T m_k - data||.  Overwrites the resident
+ * traces. */
+int psm_lsm_cg(psm_ctx *ctx, const float *data, float *image, int iters, double *resid);
+
 /* Forward-kernel variants: f32x2-packed or scalar FP32 arithmetic for each pair of 32-sample
  * blocks, and 2 or 4 blocks behind one warp-uniform skip test.  All give the same masks and
  * the same terms; they differ in instruction count.  PSM_FWD_DEFAULT lets the library pick

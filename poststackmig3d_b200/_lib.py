@@ -53,6 +53,8 @@ _CUDA_SYMBOLS = [
     ("psm_stream", ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     ("psm_count_terms", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     ("psm_count_terms_rows", ctypes.c_int, [_P, _P]),
+    ("psm_adjoint", ctypes.c_int, [_P, _P, _P]),
+    ("psm_lsm_cg", ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P]),
     ("psm_set_variant", ctypes.c_int, [_P, ctypes.c_int]),
     ("psm_get_variant", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     ("psm_autotune", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_int)]),

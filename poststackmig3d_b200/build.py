@@ -26,7 +26,12 @@ CXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SRC = [os.path.join(CSRC, "psm_cuda.cu")]
-CUDA_DEPS = CUDA_SRC + [os.path.join(CSRC, "psm_kernels.cuh"), os.path.join(INC, "psm.h")]
+CUDA_DEPS = CUDA_SRC + [os.path.join(CSRC, "psm_kernels.cuh"), os.path.join(CSRC, "psm_adjoint.cuh"),
+                         os.path.join(INC, "psm.h")]
+# Flush-to-zero: the reference's -ffast-math build runs with FTZ/DAZ set (GCC links
+# crtfastmath), and without it every rsqrt carries a subnormal fix-up.  Divisions and square
+# roots that must round like the reference use the explicit __f*_rn intrinsics.
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-ftz=true"]
 HOST_SRC = [os.path.join(CSRC, "host", f) for f in
             ("config.cpp", "segy.cpp", "velocity.cpp", "driver.cpp", "host_abi.cpp")]
 HOST_DEPS = HOST_SRC + [os.path.join(CSRC, "host", "host.hpp"),
@@ -50,8 +55,8 @@ def build_cuda(force: bool = False, extra=()) -> str:
     os.makedirs(LIB, exist_ok=True)
     out = os.path.join(LIB, "libpsm_cuda.so")
     if force or extra or _stale(out, CUDA_DEPS):
-        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-shared", f"-I{INC}", *extra, "-o", out, *CUDA_SRC])
+        _run([NVCC, *ARCH, *NVCC_FLAGS, "-Xcompiler", "-fPIC", "-shared", f"-I{INC}", *extra,
+              "-o", out, *CUDA_SRC])
     return out
 
 

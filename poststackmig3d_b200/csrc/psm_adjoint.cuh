@@ -1,0 +1,488 @@
+// Adjoint of the migration operator (demigration / spray), sm_100a.
+//
+// The forward kernel computes, for every passing term, val = fma(frac, d[lo+1]-d[lo], d[lo])
+// = (1 - frac) d[lo] + frac d[lo+1], weighted by q K (q = dt/t, K = inv_dt / v^2, or 1 with
+// amplitude correction off) and summed into the output sample.  Its transpose spreads each
+// image sample m back along the same hyperbolae:
+//     d[lo]   += (1 - frac) * q K m        d[lo+1] += frac * q K m
+// for exactly the same terms (same masks B, same travel time, same frac and q), so the pair
+// passes the dot-product test to FP32 summation noise.
+//
+// Same tile decomposition as fwd_kernel.  The producer stages no data: each ring stage is a
+// zeroed shared-memory accumulator holding one fp32 window per listed trace; consumers add
+// into it with shared-memory atomics; once a stage is released, the producer adds every
+// window into the data cube in HBM with a TMA bulk reduction (cp.reduce.async.bulk .add.f32)
+// and waits for the reduction to have read the stage before zeroing and reusing it.
+#pragma once
+
+#include "psm_kernels.cuh"
+
+namespace psm {
+
+struct AdjParams {
+    FwdParams F;          // geometry, tables, constants (F.pairs unused)
+    const float* image;   // [n_jobs][n_ox][n_t]: image of each job (duplicate rows folded)
+    float* data;          // [n_ci][n_cx][ns] accumulated in place (zero it first)
+};
+
+struct AdjMeta {
+    int count;         // windows in this stage, -1 = end of stream
+    int pad[3];
+    int4 m[kMaxG];     // crossline, dx^2 (bits), window base (smem bytes), window start (f32)
+    float shi[kMaxG];  // largest s whose lo and lo + 1 stay inside the window
+    int4 g[kMaxG];     // flush: cube row, crossline, window start, window length (samples)
+};
+
+struct AdjLayout {
+    unsigned full, empty, meta, stats, inl_klo, inl_pre, inl_dx2, stage, total;
+};
+
+// fp32 windows: cap counts 4-byte samples per stage
+__host__ __device__ inline AdjLayout adj_layout(int max_inl, int cap) {
+    AdjLayout L;
+    unsigned o = 0;
+    L.full = o;
+    o += 8 * kStages;
+    L.empty = o;
+    o += 8 * kStages;
+    L.meta = o = (o + 15) & ~15u;
+    o += sizeof(AdjMeta) * kStages;
+    L.stats = o;
+    o += sizeof(TileStats) * kTX;
+    L.inl_klo = o;
+    o += 4 * max_inl;
+    L.inl_pre = o;
+    o += 4 * (max_inl + 1);
+    L.inl_dx2 = o;
+    o += 4 * max_inl;
+    L.stage = o = (o + 127) & ~127u;
+    o += 4u * cap * kStages;
+    L.total = o;
+    return L;
+}
+
+constexpr uint32_t kMagic4 = 0x2C000000u;  // (0x4B000000 << 2) mod 2^32
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_reduce_add_f32(float* dst_global, uint32_t src_smem,
+                                                    uint32_t bytes) {
+    asm volatile(
+        "cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f32 [%0], [%1], %2;" ::"l"(
+            dst_global),
+        "r"(src_smem), "r"(bytes)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read_all() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// Producer: the fp32 window of trace (dx2, kc): samples [ws, we) cover lo and lo + 1 of every
+// passing term of the tile; ws and we multiples of 4 (16-byte bulk-copy granularity).
+__device__ __forceinline__ void adj_window(const FwdParams& P, const TileStats& S, int xa,
+                                           int xb, float dx2, int kc, int* ws_out,
+                                           int* size_out, float* shi_out) {
+    *ws_out = 0;
+    *size_out = 0;
+    *shi_out = 0.0f;
+    int lolo, lohi;
+    if (!trace_bounds(P, S, xa, xb, dx2, kc, &lolo, &lohi)) return;
+    const int ws = lolo & ~3;
+    // sample lohi + 1 <= n_t - 1 included; ns is a multiple of 8, so we <= ns
+    const int we = min((lohi + 2 + 3) & ~3, P.ns);
+    *ws_out = ws;
+    *size_out = we - ws;
+    // lo <= we - 2  <=>  s < we - 1
+    *shi_out = fminf(P.ntm1m, __uint_as_float(__float_as_uint(static_cast<float>(we - 1)) - 1u));
+}
+
+// One term of the transpose (scalar FP32): the forward's s, frac and q, then two atomic adds.
+template <bool AMP, bool MASK>
+__device__ __forceinline__ void adj_term(unsigned char* sbase, float r2, uint32_t base2,
+                                         float wsf, float shi, float T2, float F4, float BB,
+                                         float MK) {
+    const float t2 = __fmaf_rn(F4, r2, T2);
+    const float q = rsqrtf(t2);
+    const float s = fminf(fmaxf(t2 * q, wsf), shi);
+    const float mm = __fadd_rd(s, 8388608.0f);
+    const float fr = s - (mm - 8388608.0f);
+    if (MASK && !(r2 <= BB)) return;
+    const float c = AMP ? MK * q : MK;
+    const float c1 = c * fr;
+    const float c0 = c - c1;
+    float* p = reinterpret_cast<float*>(sbase + (base2 + (__float_as_uint(mm) << 2)));
+    atomicAdd(p, c0);
+    atomicAdd(p + 1, c1);
+}
+
+// Add the windows of one released stage into the data cube (one bulk reduction per window,
+// lanes in parallel) and wait until they have read shared memory.
+__device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
+                                          uint32_t smem_abs, int lane) {
+    fence_proxy_async_smem();  // the consumers' shared-memory adds -> the async proxy
+    for (int k = lane; k < m.count; k += 32) {
+        const int4 gg = m.g[k];  // row, crossline, ws, size
+        const uint32_t rel = static_cast<uint32_t>(m.m[k].z) + 4u * gg.z + kMagic4;
+        bulk_reduce_add_f32(
+            A.data + (static_cast<size_t>(gg.x) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
+            smem_abs + rel, 4u * gg.w);
+    }
+    bulk_commit();
+    bulk_wait_read_all();
+    __syncwarp();
+}
+
+template <bool AMP>
+__global__ void __launch_bounds__(32 * (kTX + 1), 2) adj_kernel(const AdjParams A) {
+    const FwdParams& P = A.F;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const AdjLayout L = adj_layout(P.max_inl, P.stage_cap);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + L.full);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem_raw + L.empty);
+    AdjMeta* meta = reinterpret_cast<AdjMeta*>(smem_raw + L.meta);
+    TileStats* wstats = reinterpret_cast<TileStats*>(smem_raw + L.stats);
+    const uint32_t smem_abs = smem_u32(smem_raw);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int jobi = blockIdx.z;
+    const Job job = P.jobs[jobi];
+    const int x0 = blockIdx.x * kTX;
+    const int T0 = blockIdx.y * kTT;
+
+    float T2[kJ], F4[kJ], BB[kJ], MK[kJ];
+    float gmax[2], gmin[2];
+    float warpmax = -1.0f;
+    const int x = x0 + warp - 1;
+    const int xv = x + P.xoff;
+    if (warp > 0) {
+        const bool xvalid = x < P.n_ox && xv >= 0 && xv < P.n_vx;
+        const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
+                                    (xvalid ? xv : 0)) * P.n_t;
+        const float* mp = A.image + (static_cast<size_t>(jobi) * P.n_ox +
+                                     (x < P.n_ox ? x : 0)) * P.n_t;
+        float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
+#pragma unroll
+        for (int j = 0; j < kJ; ++j) {
+            const int t = T0 + 32 * j + lane;
+            float v = 0.0f, t0v = 0.0f, mv = 0.0f;
+            if (xvalid && t < P.n_t) {
+                v = __ldg(vp + t);
+                t0v = __ldg(P.t0 + t);
+                mv = __ldg(mp + t);
+            }
+            const PointConst pc = point_const(v, t0v, P.tan2);
+            const float b = pass_bound(pc, P.inv_dt, P.ntm1f);
+            T2[j] = 1.0f;
+            F4[j] = 0.0f;
+            MK[j] = 0.0f;
+            if (b >= 0.0f) {
+                T2[j] = pc.t0sq * P.idt2;
+                F4[j] = pc.f4 * P.idt2;
+                MK[j] = AMP ? mv * __fdiv_rn(P.inv_dt, __fmul_rn(v, v)) : mv;
+                vmin = fminf(vmin, v);
+                vmax = fmaxf(vmax, v);
+                bmax = fmaxf(bmax, b);
+                t0min = fminf(t0min, t0v);
+                t0max = fmaxf(t0max, t0v);
+            }
+            BB[j] = b;
+        }
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+            float mx = BB[4 * g], mn = BB[4 * g];
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                mx = fmaxf(mx, BB[4 * g + k]);
+                mn = fminf(mn, BB[4 * g + k]);
+            }
+            gmax[g] = warp_max(mx);
+            gmin[g] = warp_min(mn);
+            warpmax = fmaxf(warpmax, gmax[g]);
+        }
+        vmin = warp_min(vmin);
+        vmax = warp_max(vmax);
+        bmax = warp_max(bmax);
+        t0min = warp_min(t0min);
+        t0max = warp_max(t0max);
+        if (lane == 0) {
+            TileStats s;
+            s.vmin = vmin;
+            s.vmax = vmax;
+            s.bmax = bmax;
+            s.t0min = t0min;
+            s.t0max = t0max;
+            s.any = bmax >= 0.0f;
+            wstats[warp - 1] = s;
+        }
+    } else if (lane == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kTX);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    if (warp == 0) {
+        // ---------------------------------------------------------------- producer
+        TileStats S;
+        S.vmin = 3.0e38f;
+        S.vmax = 0.0f;
+        S.bmax = -1.0f;
+        S.t0min = 3.0e38f;
+        S.t0max = 0.0f;
+        S.any = 0;
+        for (int w = 0; w < kTX; ++w) {
+            const TileStats s = wstats[w];
+            if (!s.any) continue;
+            S.any = 1;
+            S.vmin = fminf(S.vmin, s.vmin);
+            S.vmax = fmaxf(S.vmax, s.vmax);
+            S.bmax = fmaxf(S.bmax, s.bmax);
+            S.t0min = fminf(S.t0min, s.t0min);
+            S.t0max = fmaxf(S.t0max, s.t0max);
+        }
+        const int xa = max(x0 + P.xoff, 0);
+        const int xb = min(min(x0 + kTX, P.n_ox) - 1 + P.xoff, P.n_vx - 1);
+        int* inl_klo = reinterpret_cast<int*>(smem_raw + L.inl_klo);
+        int* inl_pre = reinterpret_cast<int*>(smem_raw + L.inl_pre);
+        float* inl_dx2 = reinterpret_cast<float*>(smem_raw + L.inl_dx2);
+        const int n_inl = max(job.i1 - job.i0, 0);
+        int total = 0;
+        if (S.any && xa <= xb) {
+            for (int base = 0; base < n_inl; base += 32) {
+                const int n = base + lane;
+                int cnt = 0, klo = 0;
+                float dx2 = 0.0f;
+                if (n < n_inl) {
+                    dx2 = inline_dx2(__ldg(P.il_pos + job.i0 + n), job.pos, P.d_il);
+                    if (dx2 <= S.bmax) {
+                        const int K =
+                            static_cast<int>(sqrtf(fmaxf(S.bmax - dx2, 0.0f)) * P.inv_dxl) + 2;
+                        klo = max(0, xa - K);
+                        cnt = max(0, min(P.n_cx - 1, xb + K) - klo + 1);
+                    }
+                    inl_klo[n] = klo;
+                    inl_dx2[n] = dx2;
+                }
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                if (n < n_inl) inl_pre[n] = total + incl - cnt;
+                total += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) inl_pre[n_inl] = total;
+            __syncwarp();
+        }
+        uint32_t it = 0;
+        bool alive = true;
+        int f = 0;
+        while (f < total && alive) {
+            const int idx = f + lane;
+            int ws = 0, size = 0, kc = 0, row = 0;
+            float dx2 = 0.0f, shi = 0.0f;
+            if (idx < total) {
+                int lo = 0, hi = n_inl - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (inl_pre[mid] <= idx)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                kc = inl_klo[lo] + (idx - inl_pre[lo]);
+                dx2 = inl_dx2[lo];
+                row = job.i0 + lo;
+                adj_window(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
+            }
+            int cum = size;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, cum, o);
+                if (lane >= o) cum += v;
+            }
+            const bool take = cum <= P.stage_cap;
+            const unsigned takemask = __ballot_sync(0xffffffffu, take);
+            const int consumed = __popc(takemask);
+            const unsigned nzmask = __ballot_sync(0xffffffffu, take && size > 0);
+            const int n = __popc(nzmask);
+            if (n > 0) {
+                const int stage = it % kStages;
+                const uint32_t par = ((it / kStages) & 1u) ^ 1u;
+                const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    alive = false;
+                    break;
+                }
+                AdjMeta& m = meta[stage];
+                if (it >= static_cast<uint32_t>(kStages)) adj_flush(A, m, smem_abs, lane);
+                const int tot = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
+                // zero the accumulator region of the new windows (16 B per lane per step)
+                float4* z = reinterpret_cast<float4*>(smem_raw + L.stage +
+                                                      4u * stage * P.stage_cap);
+                for (int k = lane; k < tot / 4; k += 32) z[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                const uint32_t dst_rel =
+                    L.stage + (static_cast<uint32_t>(stage) * P.stage_cap + (cum - size)) * 4u;
+                if (take && size > 0) {
+                    const int slot = __popc(nzmask & ((1u << lane) - 1u));
+                    m.m[slot] = make_int4(kc, __float_as_int(dx2),
+                                          static_cast<int>(dst_rel - 4u * ws - kMagic4),
+                                          __float_as_int(static_cast<float>(ws)));
+                    m.shi[slot] = shi;
+                    m.g[slot] = make_int4(row, kc, ws, size);
+                }
+                if (lane == 0) m.count = n;
+                __threadfence_block();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&full[stage]);
+                ++it;
+            }
+            f += consumed;
+        }
+        if (alive) {
+            // end-of-stream marker in the next stage, after flushing that stage's last use
+            const int stage = it % kStages;
+            const uint32_t par = ((it / kStages) & 1u) ^ 1u;
+            const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
+            if (__shfl_sync(0xffffffffu, ok, 0)) {
+                if (it >= static_cast<uint32_t>(kStages)) adj_flush(A, meta[stage], smem_abs, lane);
+                if (lane == 0) {
+                    meta[stage].count = -1;
+                    __threadfence_block();
+                    mbar_arrive(&full[stage]);
+                }
+                // the other stage's last use (iteration it - 1), once the consumers release it
+                if (it >= 1) {
+                    const uint32_t last = it - 1;
+                    const int s2 = last % kStages;
+                    const uint32_t par2 = (last / kStages) & 1u;
+                    const int ok2 = lane == 0 ? mbar_wait(&empty[s2], par2, P.err) : 0;
+                    if (__shfl_sync(0xffffffffu, ok2, 0)) adj_flush(A, meta[s2], smem_abs, lane);
+                }
+            }
+        }
+        bulk_wait_all();  // every reduction complete before the CTA retires
+        return;
+    }
+
+    // -------------------------------------------------------------------- consumers
+    uint32_t it = 0;
+    while (true) {
+        const int stage = it % kStages;
+        const uint32_t par = (it / kStages) & 1u;
+        if (!mbar_wait(&full[stage], par, P.err)) break;
+        const AdjMeta& m = meta[stage];
+        const int cnt = m.count;
+        if (cnt < 0) break;
+        for (int g = 0; g < cnt; ++g) {
+            const int4 md = m.m[g];
+            const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
+            if (r2 > warpmax) continue;
+            const uint32_t base2 = static_cast<uint32_t>(md.z);
+            const float wsf = __int_as_float(md.w);
+            const float shi = m.shi[g];
+#pragma unroll
+            for (int gr = 0; gr < 2; ++gr) {
+                if (r2 <= gmax[gr]) {
+                    if (r2 <= gmin[gr]) {
+#pragma unroll
+                        for (int j = 4 * gr; j < 4 * gr + 4; ++j)
+                            adj_term<AMP, false>(smem_raw, r2, base2, wsf, shi, T2[j], F4[j],
+                                                 BB[j], MK[j]);
+                    } else {
+#pragma unroll
+                        for (int j = 4 * gr; j < 4 * gr + 4; ++j)
+                            adj_term<AMP, true>(smem_raw, r2, base2, wsf, shi, T2[j], F4[j],
+                                                BB[j], MK[j]);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stage]);
+        ++it;
+    }
+}
+
+// Sum the image rows that repeat one migrated inline (the transpose of the forward's row
+// copies): out[job] = sum of image rows mapped to that job.
+__global__ void fold_rows_kernel(const float* __restrict__ image, const int* __restrict__ map,
+                                 const int* __restrict__ map_off, int n_jobs, size_t row,
+                                 float* __restrict__ out) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+         i < static_cast<size_t>(n_jobs) * row; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int j = static_cast<int>(i / row);
+        const size_t e = i % row;
+        float s = 0.0f;
+        for (int k = map_off[j]; k < map_off[j + 1]; ++k) s += image[map[k] * row + e];
+        out[i] = s;
+    }
+}
+
+// ----------------------------------------------------------------------------- CG (LSM)
+
+// out += <a, b> accumulated in FP64 (one atomic per block).
+__global__ void dot_kernel(const float* __restrict__ a, const float* __restrict__ b, size_t n,
+                           double* out) {
+    __shared__ double ws[32];
+    double s = 0.0;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        s += static_cast<double>(a[i]) * static_cast<double>(b[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) atomicAdd(out, s);
+    }
+}
+
+// CG scalars, FP64, on the device.  sc: [0] gamma, [1] delta = <q,q>, [2] gamma_new,
+// [3] alpha, [4] beta.
+__global__ void cg_alpha_kernel(double* sc) {
+    sc[3] = sc[1] > 0.0 ? sc[0] / sc[1] : 0.0;
+}
+__global__ void cg_beta_kernel(double* sc) {
+    sc[4] = sc[0] > 0.0 ? sc[2] / sc[0] : 0.0;
+    sc[0] = sc[2];
+}
+
+// m += alpha p (image space) and r -= alpha q (data space), alpha = sc[3].
+__global__ void cg_update_kernel(float* __restrict__ m, const float* __restrict__ p, size_t nm,
+                                 float* __restrict__ r, const float* __restrict__ q, size_t nr,
+                                 const double* sc) {
+    const float alpha = static_cast<float>(sc[3]);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < nm + nr;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        if (i < nm)
+            m[i] = fmaf(alpha, p[i], m[i]);
+        else
+            r[i - nm] = fmaf(-alpha, q[i - nm], r[i - nm]);
+    }
+}
+
+// p = s + beta p, beta = sc[4].
+__global__ void cg_direction_kernel(float* __restrict__ p, const float* __restrict__ s,
+                                    size_t n, const double* sc) {
+    const float beta = static_cast<float>(sc[4]);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        p[i] = fmaf(beta, p[i], s[i]);
+}
+
+}  // namespace psm

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "psm.h"
+#include "psm_adjoint.cuh"
 #include "psm_kernels.cuh"
 
 namespace {
@@ -153,6 +154,11 @@ struct psm_ctx {
     // data: fp32 traces [n_il][n_xl][ns] as uploaded; pairs: the (d, d[t+1]-d) cube the
     // forward kernel stages
     DevBuf data, pairs, vrms, image, d_jobs, d_jobs_all, il_pos, t0, err, count;
+    // adjoint: rows of each job (fold of duplicated output rows), image upload, job images
+    std::vector<int> fold_map, fold_off;
+    DevBuf d_fold_map, d_fold_off, img_in, fold;
+    // least-squares migration vectors: data space [n_tr][ns], image space [n_oi][n_ox][n_t]
+    DevBuf cg_d, cg_r, cg_q, cg_m, cg_s, cg_p, cg_sc, cg_hist;
 };
 
 namespace {
@@ -232,6 +238,9 @@ int psm_destroy(psm_ctx* c) {
     c->t0.release();
     c->err.release();
     c->count.release();
+    for (DevBuf* b : {&c->d_fold_map, &c->d_fold_off, &c->img_in, &c->fold, &c->cg_d, &c->cg_r,
+                      &c->cg_q, &c->cg_m, &c->cg_s, &c->cg_p, &c->cg_sc, &c->cg_hist})
+        b->release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSM_OK;
@@ -315,6 +324,23 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
     PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->il_pos.p, pos.data(), pos.size() * sizeof(int),
                                         cudaMemcpyHostToDevice, c->stream));
     PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->t0.p, t0.data(), t0.size() * sizeof(float),
+                                        cudaMemcpyHostToDevice, c->stream));
+    // adjoint: the output rows of every job (its own row, then the rows that repeat it)
+    c->fold_map.clear();
+    c->fold_off.assign(1, 0);
+    for (const Job& j : c->jobs) {
+        c->fold_map.push_back(j.row);
+        for (const auto& cp : c->copies)
+            if (cp.second == j.row) c->fold_map.push_back(cp.first);
+        c->fold_off.push_back(static_cast<int>(c->fold_map.size()));
+    }
+    PSM_CUDA_TRY(c->st, c->d_fold_map.ensure(c->fold_map.size() * sizeof(int)));
+    PSM_CUDA_TRY(c->st, c->d_fold_off.ensure(c->fold_off.size() * sizeof(int)));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_fold_map.p, c->fold_map.data(),
+                                        c->fold_map.size() * sizeof(int),
+                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_fold_off.p, c->fold_off.data(),
+                                        c->fold_off.size() * sizeof(int),
                                         cudaMemcpyHostToDevice, c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     c->have_geom = true;
@@ -443,6 +469,164 @@ int psm_forward(psm_ctx* c, float* image) {
     int r = psm_forward_async(c);
     if (r) return r;
     return psm_get_image(c, image);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------- adjoint, LSM
+
+namespace {
+
+constexpr int kAdjStageCapMin = 12288;  // fp32 samples per adjoint ring stage (48 KB)
+inline int adj_stage_cap(int ns) { return std::max(kAdjStageCapMin, ns); }
+
+inline unsigned grid_for(size_t n) {
+    return static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 8)));
+}
+
+// M^T: image rows [n_oi][n_ox][n_t] (device) -> data [n_il*n_xl][ns] (device, overwritten).
+int adjoint_dev(psm_ctx* c, const float* d_rows, float* d_out) {
+    const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    const int n_jobs = static_cast<int>(c->jobs.size());
+    const float* job_img = d_rows;  // without repeated rows, job k is output row k
+    if (!c->copies.empty()) {
+        PSM_CUDA_TRY(c->st, c->fold.ensure(static_cast<size_t>(n_jobs) * row * sizeof(float)));
+        psm::fold_rows_kernel<<<grid_for(n_jobs * row), 256, 0, c->stream>>>(
+            d_rows, c->d_fold_map.as<int>(), c->d_fold_off.as<int>(), n_jobs, row,
+            c->fold.as<float>());
+        PSM_CUDA_TRY(c->st, cudaGetLastError());
+        job_img = c->fold.as<float>();
+    }
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(d_out, 0, n_tr * c->ns * sizeof(float), c->stream));
+    psm::AdjParams A{};
+    A.F = volume_params(c);
+    A.F.stage_cap = adj_stage_cap(c->ns);
+    A.image = job_img;
+    A.data = d_out;
+    const size_t smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap).total;
+    if (smem > kMaxDynSmem)
+        return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t / aperture too large for the adjoint ring");
+    dim3 grid((c->g.n_ox + psm::kTX - 1) / psm::kTX, (c->g.n_t + psm::kTT - 1) / psm::kTT,
+              n_jobs);
+    dim3 block(32 * (psm::kTX + 1));
+    if (c->g.amp_correction) {
+        PSM_CUDA_TRY(c->st, cudaFuncSetAttribute(psm::adj_kernel<true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(smem)));
+        psm::adj_kernel<true><<<grid, block, smem, c->stream>>>(A);
+    } else {
+        PSM_CUDA_TRY(c->st, cudaFuncSetAttribute(psm::adj_kernel<false>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(smem)));
+        psm::adj_kernel<false><<<grid, block, smem, c->stream>>>(A);
+    }
+    PSM_CUDA_TRY(c->st, cudaGetLastError());
+    return PSM_OK;
+}
+
+// M: data [n_il*n_xl][ns] (device, zero tail) -> image rows (device).  Rebuilds the pair
+// cube from d_vec.
+int forward_dev(psm_ctx* c, const float* d_vec, float* d_img) {
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    PSM_CUDA_TRY(c->st, build_pairs(d_vec, c->pairs.as<float2>(), n_tr, c->ns, c->stream));
+    FwdParams P = volume_params(c);
+    P.image = d_img;
+    PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
+                                   c->g.amp_correction != 0, c->variant, c->stream));
+    const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
+    for (const auto& cp : c->copies)
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(d_img + cp.first * row, d_img + cp.second * row,
+                                            row * sizeof(float), cudaMemcpyDeviceToDevice,
+                                            c->stream));
+    return PSM_OK;
+}
+
+int dot_dev(psm_ctx* c, const float* a, const float* b, size_t n, double* out) {
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(out, 0, sizeof(double), c->stream));
+    psm::dot_kernel<<<grid_for(n), 256, 0, c->stream>>>(a, b, n, out);
+    PSM_CUDA_TRY(c->st, cudaGetLastError());
+    return PSM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psm_adjoint(psm_ctx* c, const float* image, float* data) {
+    if (!c || !image || !data) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry and vrms must be set");
+    cudaSetDevice(c->device);
+    const size_t n_img = static_cast<size_t>(c->g.n_oi) * c->g.n_ox * c->g.n_t;
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    PSM_CUDA_TRY(c->st, c->img_in.ensure(n_img * sizeof(float)));
+    PSM_CUDA_TRY(c->st, c->cg_q.ensure(n_tr * c->ns * sizeof(float)));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->img_in.p, image, n_img * sizeof(float),
+                                        cudaMemcpyHostToDevice, c->stream));
+    int r = adjoint_dev(c, c->img_in.as<float>(), c->cg_q.as<float>());
+    if (r) return r;
+    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(data, c->g.n_t * sizeof(float), c->cg_q.p,
+                                          c->ns * sizeof(float), c->g.n_t * sizeof(float), n_tr,
+                                          cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int psm_lsm_cg(psm_ctx* c, const float* data, float* image, int iters, double* resid) {
+    if (!c || !data || !image || iters < 0) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry and vrms must be set");
+    cudaSetDevice(c->device);
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    const size_t nd = n_tr * c->ns;
+    const size_t nm = static_cast<size_t>(c->g.n_oi) * c->g.n_ox * c->g.n_t;
+    cudaStream_t s = c->stream;
+    for (DevBuf* b : {&c->cg_d, &c->cg_r, &c->cg_q})
+        PSM_CUDA_TRY(c->st, b->ensure(nd * sizeof(float)));
+    for (DevBuf* b : {&c->cg_m, &c->cg_s, &c->cg_p})
+        PSM_CUDA_TRY(c->st, b->ensure(nm * sizeof(float)));
+    PSM_CUDA_TRY(c->st, c->cg_sc.ensure(8 * sizeof(double)));
+    PSM_CUDA_TRY(c->st, c->cg_hist.ensure((iters + 1) * sizeof(double)));
+    float *d = c->cg_d.as<float>(), *r = c->cg_r.as<float>(), *q = c->cg_q.as<float>();
+    float *m = c->cg_m.as<float>(), *sv = c->cg_s.as<float>(), *p = c->cg_p.as<float>();
+    double *sc = c->cg_sc.as<double>(), *hist = c->cg_hist.as<double>();
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), s));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(d, 0, nd * sizeof(float), s));
+    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(d, c->ns * sizeof(float), data,
+                                          c->g.n_t * sizeof(float), c->g.n_t * sizeof(float),
+                                          n_tr, cudaMemcpyHostToDevice, s));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(r, d, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(m, 0, nm * sizeof(float), s));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
+    int rc;
+    // CGLS: r = d - M^T m, s = M r, p = s, gamma = <s, s>
+    if ((rc = dot_dev(c, r, r, nd, hist))) return rc;
+    if ((rc = forward_dev(c, r, sv))) return rc;
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p, sv, nm * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    if ((rc = dot_dev(c, sv, sv, nm, sc + 0))) return rc;
+    for (int k = 0; k < iters; ++k) {
+        if ((rc = adjoint_dev(c, p, q))) return rc;                   // q = M^T p
+        if ((rc = dot_dev(c, q, q, nd, sc + 1))) return rc;           // delta
+        psm::cg_alpha_kernel<<<1, 1, 0, s>>>(sc);                     // alpha = gamma / delta
+        psm::cg_update_kernel<<<grid_for(nm + nd), 256, 0, s>>>(m, p, nm, r, q, nd, sc);
+        if ((rc = dot_dev(c, r, r, nd, hist + k + 1))) return rc;     // ||r||^2
+        if ((rc = forward_dev(c, r, sv))) return rc;                  // s = M r
+        if ((rc = dot_dev(c, sv, sv, nm, sc + 2))) return rc;         // gamma_new
+        psm::cg_beta_kernel<<<1, 1, 0, s>>>(sc);                      // beta, gamma
+        psm::cg_direction_kernel<<<grid_for(nm), 256, 0, s>>>(p, sv, nm, sc);  // p = s + beta p
+        PSM_CUDA_TRY(c->st, cudaGetLastError());
+    }
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image, m, nm * sizeof(float), cudaMemcpyDeviceToHost, s));
+    std::vector<double> h(iters + 1);
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(h.data(), hist, (iters + 1) * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
+    c->have_traces = false;  // the pair cube now holds the last residual
+    if (resid)
+        for (int k = 0; k <= iters; ++k) resid[k] = std::sqrt(std::max(h[k], 0.0));
+    return read_device_error(c);
 }
 
 int psm_count_terms_rows(psm_ctx* c, int64_t* per_row) {

@@ -299,23 +299,20 @@ __global__ void pair_kernel(const float* __restrict__ src, float2* __restrict__ 
 
 // ----------------------------------------------------------------------------- forward
 
-// Producer: the window of trace (dx2, kc) for the tile.  size 0: the trace has no term that
-// passes the masks.  ws is even and size even (16-byte TMA granularity for 8-byte samples).
+// Producer: lo of every passing term of the tile on trace (dx2, kc) lies in [*lolo, *lohi]
+// (with two samples of slack for rounding); false when the trace has no passing term.
 // Bounds: t >= t0 and, inside the aperture r <= v t0 tan/2, t0 >= 2 r_min / (v_max tan);
 // t^2 = t0^2 + f4 r^2 <= min(t0max^2 + 4 r_max^2 / v_min^2, t0max^2 (1 + tan^2)).
-__device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats& S, int xa,
-                                             int xb, float dx2, int kc, int* ws_out,
-                                             int* size_out, float* shi_out) {
-    *ws_out = 0;
-    *size_out = 0;
-    *shi_out = 0.0f;
+__device__ __forceinline__ bool trace_bounds(const FwdParams& P, const TileStats& S, int xa,
+                                             int xb, float dx2, int kc, int* lolo_out,
+                                             int* lohi_out) {
     const int dkmin = kc < xa ? xa - kc : (kc > xb ? kc - xb : 0);
     const int dkmax = max(abs(kc - xa), abs(kc - xb));
     const float dymin = static_cast<float>(dkmin) * P.d_xl;
     const float dymax = static_cast<float>(dkmax) * P.d_xl;
     const float rmin2 = fmaf(dymin, dymin, dx2);
     const float rmax2 = fmaf(dymax, dymax, dx2);
-    if (rmin2 > S.bmax * 1.0001f + 1e-6f) return;
+    if (rmin2 > S.bmax * 1.0001f + 1e-6f) return false;
     float t0lo = S.t0min;
     if (P.tanth > 0.0f) t0lo = fmaxf(t0lo, 2.0f * sqrtf(rmin2) / (S.vmax * P.tanth));
     const float tlo = sqrtf(fmaf(t0lo, t0lo, 4.0f * rmin2 / fmaf(S.vmax, S.vmax, 1e-10f)));
@@ -324,9 +321,22 @@ __device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats
               S.t0max * S.t0max * (1.0f + P.tan2) * 1.0001f);
     const float slo = tlo * P.inv_dt;
     const float shi = fminf(sqrtf(thi2) * P.inv_dt, 1.0e9f);
-    const int lolo = max(static_cast<int>(floorf(slo)) - 2, 0);
-    const int lohi = min(static_cast<int>(floorf(shi)) + 2, P.n_t - 2);
-    if (lolo > lohi) return;
+    *lolo_out = max(static_cast<int>(floorf(slo)) - 2, 0);
+    *lohi_out = min(static_cast<int>(floorf(shi)) + 2, P.n_t - 2);
+    return *lolo_out <= *lohi_out;
+}
+
+// Pair window of trace (dx2, kc) for the forward kernel: pairs [ws, we) with ws and we even
+// (16-byte TMA granularity for 8-byte samples) cover lo in [lolo, lohi]; size 0 when the
+// trace has no passing term.
+__device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats& S, int xa,
+                                             int xb, float dx2, int kc, int* ws_out,
+                                             int* size_out, float* shi_out) {
+    *ws_out = 0;
+    *size_out = 0;
+    *shi_out = 0.0f;
+    int lolo, lohi;
+    if (!trace_bounds(P, S, xa, xb, dx2, kc, &lolo, &lohi)) return;
     const int ws = lolo & ~1;
     const int we = (lohi + 2) & ~1;  // pairs [ws, we) cover lo in [lolo, lohi]
     *ws_out = ws;

@@ -247,6 +247,28 @@ class Migrator:
         check(self._L.psm_count_terms(self._ctx, ctypes.byref(n)), self._err)
         return int(n.value)
 
+    def adjoint(self, image, out=None):
+        """Adjoint of forward (demigration / spray): data [n_il][n_xl][n_t] = M^T image."""
+        g = self.geom
+        if isinstance(image, np.ndarray):
+            image = _f32(image, self.image_shape())
+        if out is None:
+            out = np.empty((g.n_il, g.n_xl, g.n_t), dtype=np.float32)
+        check(self._L.psm_adjoint(self._ctx, _addr(image), _addr(out)), self._err)
+        return out
+
+    def lsm_cg(self, data, iters: int):
+        """Least-squares migration: CG on min ||M^T m - data||^2 (FP32 operators, FP64
+        inner products on the GPU).  Returns (image, data-residual norms [iters + 1])."""
+        g = self.geom
+        if isinstance(data, np.ndarray):
+            data = _f32(data, (g.n_il, g.n_xl, g.n_t))
+        img = np.empty(self.image_shape(), dtype=np.float32)
+        hist = np.zeros(iters + 1, dtype=np.float64)
+        check(self._L.psm_lsm_cg(self._ctx, _addr(data), img.ctypes.data, int(iters),
+                                 hist.ctypes.data), self._err)
+        return img, hist
+
     VARIANTS = {1: "scalar/g2", 2: "scalar/g4", 3: "packed/g2", 4: "packed/g4"}
 
     def set_variant(self, variant: int) -> None:
