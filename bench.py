@@ -154,7 +154,7 @@ class ClockSampler:
 
 def profile_traffic():
     """DRAM bytes per forward launch from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "fwd_kernel_config2.md")
+    p = os.path.join(ROOT, "profiles", "fwd_kernel_config2_201.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
