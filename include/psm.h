@@ -116,16 +116,19 @@ int psm_adjoint(psm_ctx *ctx, const float *image, float *data);
 int psm_lsm_cg(psm_ctx *ctx, const float *data, float *image, int iters, double *resid);
 
 /* Forward-kernel variants: f32x2-packed or scalar FP32 arithmetic for each pair of 32-sample
- * blocks, and 2 or 4 blocks behind one warp-uniform skip test.  All give the same masks and
- * the same terms; they differ in instruction count.  PSM_FWD_DEFAULT lets the library pick
- * (the result of psm_autotune once it has run on the ctx). */
+ * blocks, 2 or 4 blocks behind one warp-uniform skip test, and 8 or 16 blocks per lane (a
+ * tile of 256 or 512 output samples).  All give the same masks and the same terms, bit for
+ * bit; they differ in instruction count and shared-memory traffic.  PSM_FWD_DEFAULT lets the
+ * library pick (the result of psm_autotune once it has run on the ctx). */
 typedef enum {
     PSM_FWD_DEFAULT = 0,
     PSM_FWD_SCALAR_G2 = 1,
     PSM_FWD_SCALAR_G4 = 2,
     PSM_FWD_PACKED_G2 = 3,
     PSM_FWD_PACKED_G4 = 4,
-    PSM_FWD_N_VARIANTS = 5
+    PSM_FWD_PACKED_G4_J16 = 5,
+    PSM_FWD_SCALAR_G4_J16 = 6,
+    PSM_FWD_N_VARIANTS = 7
 } psm_fwd_variant;
 int psm_set_variant(psm_ctx *ctx, int variant);
 int psm_get_variant(psm_ctx *ctx, int *variant);

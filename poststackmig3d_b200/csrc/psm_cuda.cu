@@ -79,15 +79,16 @@ size_t fwd_smem(const FwdParams& P) {
     return b <= kMaxDynSmem ? b : 0;
 }
 
-template <bool AMP, bool PACKED, int GB>
+template <bool AMP, bool PACKED, int GB, int J>
 cudaError_t launch_fwd_v(const FwdParams& P, int n_jobs, size_t smem, cudaStream_t s) {
-    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + psm::kTT - 1) / psm::kTT, n_jobs);
+    constexpr int TT = 32 * J;
+    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + TT - 1) / TT, n_jobs);
     dim3 block(32 * (psm::kTX + 1));
-    cudaError_t e = cudaFuncSetAttribute(psm::fwd_kernel<AMP, PACKED, GB>,
+    cudaError_t e = cudaFuncSetAttribute(psm::fwd_kernel<AMP, PACKED, GB, J>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    psm::fwd_kernel<AMP, PACKED, GB><<<grid, block, smem, s>>>(P);
+    psm::fwd_kernel<AMP, PACKED, GB, J><<<grid, block, smem, s>>>(P);
     return cudaGetLastError();
 }
 
@@ -95,10 +96,12 @@ template <bool AMP>
 cudaError_t launch_fwd_amp(const FwdParams& P, int n_jobs, int variant, size_t smem,
                            cudaStream_t s) {
     switch (variant) {
-        case PSM_FWD_SCALAR_G2: return launch_fwd_v<AMP, false, 2>(P, n_jobs, smem, s);
-        case PSM_FWD_SCALAR_G4: return launch_fwd_v<AMP, false, 4>(P, n_jobs, smem, s);
-        case PSM_FWD_PACKED_G2: return launch_fwd_v<AMP, true, 2>(P, n_jobs, smem, s);
-        case PSM_FWD_PACKED_G4: return launch_fwd_v<AMP, true, 4>(P, n_jobs, smem, s);
+        case PSM_FWD_SCALAR_G2: return launch_fwd_v<AMP, false, 2, 8>(P, n_jobs, smem, s);
+        case PSM_FWD_SCALAR_G4: return launch_fwd_v<AMP, false, 4, 8>(P, n_jobs, smem, s);
+        case PSM_FWD_PACKED_G2: return launch_fwd_v<AMP, true, 2, 8>(P, n_jobs, smem, s);
+        case PSM_FWD_PACKED_G4: return launch_fwd_v<AMP, true, 4, 8>(P, n_jobs, smem, s);
+        case PSM_FWD_PACKED_G4_J16: return launch_fwd_v<AMP, true, 4, 16>(P, n_jobs, smem, s);
+        case PSM_FWD_SCALAR_G4_J16: return launch_fwd_v<AMP, false, 4, 16>(P, n_jobs, smem, s);
         default: return cudaErrorInvalidValue;
     }
 }

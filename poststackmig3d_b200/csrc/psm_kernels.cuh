@@ -401,12 +401,15 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
 }
 
 // Kernel variants: PACKED selects f32x2 or scalar FP32 arithmetic for a block pair; GB is
-// the number of 32-sample blocks behind one warp-uniform skip test (2 or 4).
-template <bool AMP, bool PACKED, int GB>
+// the number of 32-sample blocks behind one warp-uniform skip test (2 or 4); J the number
+// of 32-sample blocks per lane (the tile covers 32 J output samples).
+template <bool AMP, bool PACKED, int GB, int J>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
     static_assert(GB == 2 || GB == 4, "skip groups of 2 or 4 blocks");
-    constexpr int NG = kJ / GB;  // skip groups per lane
+    static_assert(J % GB == 0, "whole skip groups per lane");
+    constexpr int NG = J / GB;   // skip groups per lane
     constexpr int PG = GB / 2;   // block pairs per group
+    constexpr int TT = 32 * J;   // output samples per tile
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + L.full);
@@ -419,10 +422,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
     const int lane = threadIdx.x & 31;
     const Job job = P.jobs[blockIdx.z];
     const int x0 = blockIdx.x * kTX;
-    const int T0 = blockIdx.y * kTT;
+    const int T0 = blockIdx.y * TT;
 
-    // ---- consumers: per-sample constants (4 register pairs) and tile statistics
-    float2 T2[kJ / 2], F4[kJ / 2], BB[kJ / 2], ACC[kJ / 2];
+    // ---- consumers: per-sample constants (J / 2 register pairs) and tile statistics
+    float2 T2[J / 2], F4[J / 2], BB[J / 2], ACC[J / 2];
     float gmax[NG], gmin[NG];
     float warpmax = -1.0f;
     const int x = x0 + warp - 1;
@@ -432,9 +435,9 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
         const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
                                     (xvalid ? xv : 0)) * P.n_t;
         float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
-        float bj[kJ];
+        float bj[J];
 #pragma unroll
-        for (int j = 0; j < kJ; ++j) {
+        for (int j = 0; j < J; ++j) {
             const int t = T0 + 32 * j + lane;
             float v = 0.0f, t0v = 0.0f;
             if (xvalid && t < P.n_t) {
@@ -465,7 +468,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
             }
         }
 #pragma unroll
-        for (int p = 0; p < kJ / 2; ++p) ACC[p] = make_float2(0.0f, 0.0f);
+        for (int p = 0; p < J / 2; ++p) ACC[p] = make_float2(0.0f, 0.0f);
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
             float mx = bj[GB * g], mn = bj[GB * g];
@@ -686,7 +689,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
                                     (xvalid ? xv : 0)) * P.n_t;
         float* op = P.image + (static_cast<size_t>(job.row) * P.n_ox + x) * P.n_t;
 #pragma unroll
-        for (int j = 0; j < kJ; ++j) {
+        for (int j = 0; j < J; ++j) {
             const int t = T0 + 32 * j + lane;
             if (t < P.n_t) {
                 const float b = (j & 1) ? BB[j >> 1].y : BB[j >> 1].x;

@@ -269,7 +269,8 @@ class Migrator:
                                  hist.ctypes.data), self._err)
         return img, hist
 
-    VARIANTS = {1: "scalar/g2", 2: "scalar/g4", 3: "packed/g2", 4: "packed/g4"}
+    VARIANTS = {1: "scalar/g2", 2: "scalar/g4", 3: "packed/g2", 4: "packed/g4",
+                5: "packed/g4/j16", 6: "scalar/g4/j16"}
 
     def set_variant(self, variant: int) -> None:
         check(self._L.psm_set_variant(self._ctx, int(variant)), self._err)
@@ -282,7 +283,7 @@ class Migrator:
     def autotune(self):
         """Time every forward variant once on the resident cube and keep the fastest.
         Returns (best variant, {variant: ms})."""
-        ms = np.zeros(5, dtype=np.float32)
+        ms = np.zeros(max(self.VARIANTS) + 1, dtype=np.float32)
         best = ctypes.c_int()
         check(self._L.psm_autotune(self._ctx, ms.ctypes.data, ctypes.byref(best)), self._err)
         return best.value, {v: float(ms[v]) for v in self.VARIANTS}
