@@ -20,6 +20,7 @@ Multi-GPU (torchrun): independent replicas, one per GPU, no collective on the da
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import datetime
 import json
 import os
@@ -58,6 +59,10 @@ def parse():
     p.add_argument("--cpu-rows", type=int, default=2,
                    help="output inlines in the bounded CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
+                   help="trace storage in HBM (16-bit: per-trace fp32 scale, fp32 sums)")
+    p.add_argument("--compensated", action="store_true",
+                   help="compensated (Kahan) summation over the aperture")
     return p.parse_args()
 
 
@@ -83,7 +88,7 @@ def config_dict(W, g, extra=None):
                      f"{W.angle:.0f} deg aperture, amp {'on' if W.amp else 'off'}, "
                      f"pad {W.pad_il}/{W.pad_xl}",
          "traces": [g.n_il, g.n_xl], "samples": g.n_t, "image": [g.n_oi, g.n_ox, g.n_t],
-         "m_il": g.m_il, "storage": "f32",
+         "m_il": g.m_il, "storage": g.precision, "compensated": bool(g.compensated),
          "l2": "inputs larger than L2 (cube 644 MB, Vrms 644 MB)"}
     if extra:
         d.update(extra)
@@ -269,7 +274,8 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
 
     W = workload(args.workload)
-    g = geometry(W)
+    g = dataclasses.replace(geometry(W), precision=args.storage,
+                            compensated=bool(args.compensated))
     m = Migrator(local)
     m.set_geometry(g)
     m.set_traces(W.data)
@@ -363,7 +369,8 @@ def run_ours(args):
     hbm_ach = comp_bytes / (ms * 1e-3) / 1e9
     roofline = {
         "bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gterm/s",
-        "frac": achieved / peak, "traffic": profile_traffic(),
+        "frac": achieved / peak,
+        "traffic": profile_traffic() if g.precision == "f32" and not g.compensated else None,
         "peak_basis": f"{TERMS_PER_CLK_SM:.0f} terms/clk/SM (SFU, FP32, LDS limbs) x {N_SM} "
                       f"SMs x median SM clock {sm_mhz:.0f} MHz under load",
         "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",

@@ -43,7 +43,13 @@ typedef enum { PSM_F32 = 0, PSM_BF16 = 1, PSM_F16 = 2 } psm_precision;
  *   pad_il, pad_xl    inline_padding / crossline_padding
  *   n_oi, n_ox        output inlines / crosslines (labels padded by main.cpp:144-172)
  *   amp_correction    1/(t v^2) weighting on/off
- *   precision         storage of the traces in HBM (psm_precision)
+ *   precision         storage of the traces in HBM (psm_precision): PSM_F32 keeps the
+ *                     reference's fp32 samples; PSM_BF16 / PSM_F16 keep each trace as 16-bit
+ *                     values d / scale with one fp32 scale per trace (scale = max |d|), and
+ *                     sum in fp32.  No counterpart in the reference (fp32 only).
+ *   compensated       nonzero: compensated (Kahan) summation over the aperture, partial
+ *                     sums of at most 32 traces added with Kahan's compensation.  No
+ *                     counterpart in the reference (plain fp32 sum, migration_kernel.cpp:229).
  */
 typedef struct {
     int32_t n_il, n_xl, n_t;
@@ -56,6 +62,7 @@ typedef struct {
     float d_il, d_xl;
     float tan2_theta;
     double dt_seconds;
+    int32_t compensated;
 } psm_geom;
 
 typedef struct psm_ctx psm_ctx;

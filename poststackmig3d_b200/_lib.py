@@ -23,7 +23,8 @@ class PsmGeom(ctypes.Structure):
                 ("n_oi", ctypes.c_int32), ("n_ox", ctypes.c_int32), ("m_il", ctypes.c_int32),
                 ("amp_correction", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("dt", ctypes.c_float), ("d_il", ctypes.c_float), ("d_xl", ctypes.c_float),
-                ("tan2_theta", ctypes.c_float), ("dt_seconds", ctypes.c_double)]
+                ("tan2_theta", ctypes.c_float), ("dt_seconds", ctypes.c_double),
+                ("compensated", ctypes.c_int32)]
 
 
 class PsmError(RuntimeError):

@@ -1,6 +1,6 @@
 """Build recipe for the native parts of poststackmig3d_b200 (in-tree, no JIT cache).
 
-    python -m poststackmig3d_b200.build
+    python -m poststackmig3d_b200.build [--force] [--debug-bounds]
 
 produces
     poststackmig3d_b200/lib/libpsm_cuda.so   sm_100a kernels + C ABI (include/psm.h)
@@ -75,10 +75,13 @@ def build_host(force: bool = False) -> str:
     return out
 
 
-def build(force: bool = False) -> None:
-    build_cuda(force)
+def build(force: bool = False, debug_bounds: bool = False) -> None:
+    """debug_bounds: the forward kernel checks that every unclamped sample index lies inside
+    its staged window and reports PSM_ERR_DEVICE instead of reading outside it (slower;
+    for validation runs)."""
+    build_cuda(force, ["-DPSM_DEBUG_BOUNDS"] if debug_bounds else ())
     build_host(force)
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv)
+    build(force="--force" in sys.argv, debug_bounds="--debug-bounds" in sys.argv)

@@ -194,6 +194,7 @@ void run(const Config& cfg, bool verbose, Plan* plan_only) {
         g.m_il = m_il;
         g.amp_correction = cfg.amp_correction ? 1 : 0;
         g.precision = cfg.precision;
+        g.compensated = cfg.compensated ? 1 : 0;
         g.dt = static_cast<float>(dt);
         g.d_il = static_cast<float>(cfg.inline_step);
         g.d_xl = static_cast<float>(cfg.crossline_step);

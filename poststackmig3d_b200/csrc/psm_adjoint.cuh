@@ -164,8 +164,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) adj_kernel(const AdjParams 
     const int xv = x + P.xoff;
     if (warp > 0) {
         const bool xvalid = x < P.n_ox && xv >= 0 && xv < P.n_vx;
-        const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
-                                    (xvalid ? xv : 0)) * P.n_t;
+        const float* vp = vrms_trace(P, job.vrow, xvalid ? xv : 0);
         const float* mp = A.image + (static_cast<size_t>(jobi) * P.n_ox +
                                      (x < P.n_ox ? x : 0)) * P.n_t;
         float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;

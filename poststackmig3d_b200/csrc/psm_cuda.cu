@@ -26,8 +26,17 @@ constexpr size_t kMaxDynSmem = 232448;  // 227 KB per CTA on sm_100
 // the TMA bulk copies; the tail samples stay zero.
 inline int trace_stride(int n_t) { return (n_t + 7) & ~7; }
 
-// Ring stage capacity (samples): at least one whole trace so a stage always takes a window.
-inline int stage_cap(int ns) { return std::max(psm::kStageCapMin, ns); }
+// Ring stage capacity (samples): 48 KB a stage, and at least one whole trace so a stage
+// always takes a window.
+inline int stage_cap(int ns, int store = psm::kStoreF32) {
+    return std::max(psm::kStageCapMin * 8 / psm::store_bytes(store), ns);
+}
+
+// Storage of a geometry's traces (psm_precision -> psm::kStore*).
+inline int store_of(int precision) {
+    return precision == PSM_BF16 ? psm::kStoreBF16
+                                 : precision == PSM_F16 ? psm::kStoreF16 : psm::kStoreF32;
+}
 
 int max_inline_window(const std::vector<Job>& jobs) {
     int m = 1;
@@ -74,22 +83,32 @@ struct Status {
     } while (0)
 
 // Dynamic shared memory of a forward launch (0: too large for one CTA).
-size_t fwd_smem(const FwdParams& P) {
-    const size_t b = psm::smem_layout(P.max_inl, P.stage_cap).total;
+size_t fwd_smem(const FwdParams& P, int store = psm::kStoreF32) {
+    const size_t b = psm::smem_layout(P.max_inl, P.stage_cap, psm::store_bytes(store)).total;
     return b <= kMaxDynSmem ? b : 0;
 }
 
-template <bool AMP, bool PACKED, int GB, int J>
+template <bool AMP, bool PACKED, int GB, int J, int STORE = psm::kStoreF32, bool KAHAN = false>
 cudaError_t launch_fwd_v(const FwdParams& P, int n_jobs, size_t smem, cudaStream_t s) {
     constexpr int TT = 32 * J;
+    auto* kern = psm::fwd_kernel<AMP, PACKED, GB, J, STORE, KAHAN>;
     dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + TT - 1) / TT, n_jobs);
     dim3 block(32 * (psm::kTX + 1));
-    cudaError_t e = cudaFuncSetAttribute(psm::fwd_kernel<AMP, PACKED, GB, J>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    psm::fwd_kernel<AMP, PACKED, GB, J><<<grid, block, smem, s>>>(P);
+    kern<<<grid, block, smem, s>>>(P);
     return cudaGetLastError();
+}
+
+// 16-bit storage and compensated summation: the packed kernel with skip groups of 4, with
+// 8 or 16 blocks a lane (8 only with compensation: its partial and compensation registers
+// leave no room for 16).
+template <bool AMP, int STORE, bool KAHAN>
+cudaError_t launch_fwd_sk(const FwdParams& P, int n_jobs, bool j16, size_t smem,
+                          cudaStream_t s) {
+    if (!KAHAN && j16) return launch_fwd_v<AMP, true, 4, 16, STORE, false>(P, n_jobs, smem, s);
+    return launch_fwd_v<AMP, true, 4, 8, STORE, KAHAN>(P, n_jobs, smem, s);
 }
 
 template <bool AMP>
@@ -108,14 +127,60 @@ cudaError_t launch_fwd_amp(const FwdParams& P, int n_jobs, int variant, size_t s
 
 constexpr int kDefaultVariant = PSM_FWD_PACKED_G4;
 
-// Launch the forward kernel for n_jobs jobs (P.max_inl and P.stage_cap set).
-cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, int variant, cudaStream_t s) {
-    if (n_jobs <= 0 || P.n_ox <= 0 || P.n_t <= 0) return cudaSuccess;
-    const size_t smem = fwd_smem(P);
-    if (!smem) return cudaErrorInvalidValue;
+inline bool is_j16(int variant) {
+    return variant == PSM_FWD_PACKED_G4_J16 || variant == PSM_FWD_SCALAR_G4_J16;
+}
+
+// The variant that actually runs: 16-bit storage runs the packed skip-4 kernel with the
+// variant's blocks per lane, compensated summation the packed skip-4 kernel with 8.
+inline int effective_variant(int variant, int store, bool kahan) {
     if (variant == PSM_FWD_DEFAULT) variant = kDefaultVariant;
-    return amp ? launch_fwd_amp<true>(P, n_jobs, variant, smem, s)
-               : launch_fwd_amp<false>(P, n_jobs, variant, smem, s);
+    if (store == psm::kStoreF32 && !kahan) return variant;
+    return !kahan && is_j16(variant) ? PSM_FWD_PACKED_G4_J16 : PSM_FWD_PACKED_G4;
+}
+
+template <bool AMP>
+cudaError_t launch_fwd_mode(const FwdParams& P, int n_jobs, int variant, int store, bool kahan,
+                            size_t smem, cudaStream_t s) {
+    const bool j16 = is_j16(variant);
+    switch (store * 2 + (kahan ? 1 : 0)) {
+        case psm::kStoreF32 * 2: return launch_fwd_amp<AMP>(P, n_jobs, variant, smem, s);
+        case psm::kStoreF32 * 2 + 1:
+            return launch_fwd_sk<AMP, psm::kStoreF32, true>(P, n_jobs, j16, smem, s);
+        case psm::kStoreBF16 * 2:
+            return launch_fwd_sk<AMP, psm::kStoreBF16, false>(P, n_jobs, j16, smem, s);
+        case psm::kStoreBF16 * 2 + 1:
+            return launch_fwd_sk<AMP, psm::kStoreBF16, true>(P, n_jobs, j16, smem, s);
+        case psm::kStoreF16 * 2:
+            return launch_fwd_sk<AMP, psm::kStoreF16, false>(P, n_jobs, j16, smem, s);
+        case psm::kStoreF16 * 2 + 1:
+            return launch_fwd_sk<AMP, psm::kStoreF16, true>(P, n_jobs, j16, smem, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// Launch the forward kernel for n_jobs jobs (P.max_inl and P.stage_cap set; P.pairs for fp32
+// storage, P.words and P.scales for 16-bit storage).
+cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, int variant, cudaStream_t s,
+                       int store = psm::kStoreF32, bool kahan = false) {
+    if (n_jobs <= 0 || P.n_ox <= 0 || P.n_t <= 0) return cudaSuccess;
+    const size_t smem = fwd_smem(P, store);
+    if (!smem) return cudaErrorInvalidValue;
+    variant = effective_variant(variant, store, kahan);
+    return amp ? launch_fwd_mode<true>(P, n_jobs, variant, store, kahan, smem, s)
+               : launch_fwd_mode<false>(P, n_jobs, variant, store, kahan, smem, s);
+}
+
+// words[n_rows][ns] and scales[n_rows] from the fp32 rows (quantize_kernel, one warp a row).
+cudaError_t quantize(const float* src, uint32_t* words, float* scales, size_t n_rows, int ns,
+                     int store, cudaStream_t s) {
+    if (!n_rows) return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>(std::min<size_t>((n_rows + 7) / 8, 148 * 16));
+    if (store == psm::kStoreBF16)
+        psm::quantize_kernel<psm::kStoreBF16><<<blocks, 256, 0, s>>>(src, words, scales, n_rows, ns);
+    else
+        psm::quantize_kernel<psm::kStoreF16><<<blocks, 256, 0, s>>>(src, words, scales, n_rows, ns);
+    return cudaGetLastError();
 }
 
 // pairs[n_rows][ns] from the fp32 rows (pair_kernel).
@@ -137,6 +202,8 @@ void fill_consts(FwdParams& P, float dt, float d_il, float d_xl, float tan2) {
     P.tanth = std::sqrt(std::max(tan2, 0.0f));
     P.ntm1f = static_cast<float>(P.n_t) - 1.0f;
     P.ntm1m = std::nextafter(P.ntm1f, 0.0f);
+    P.vs_x = P.n_t;  // dense Vrms cube [n_vrow][n_vx][n_t]
+    P.vs_row = static_cast<long long>(P.n_vx) * P.n_t;
 }
 
 }  // namespace
@@ -150,6 +217,7 @@ struct psm_ctx {
     bool have_geom = false, have_traces = false, have_vrms = false;
     psm_geom g{};
     int ns = 0;
+    int store = psm::kStoreF32;  // trace storage of the resident cube
     int variant = PSM_FWD_DEFAULT;
     std::vector<Job> jobs;       // one per distinct migrated inline
     std::vector<Job> jobs_all;   // one per output row (term counting)
@@ -157,6 +225,8 @@ struct psm_ctx {
     // data: fp32 traces [n_il][n_xl][ns] as uploaded; pairs: the (d, d[t+1]-d) cube the
     // forward kernel stages
     DevBuf data, pairs, vrms, image, d_jobs, d_jobs_all, il_pos, t0, err, count;
+    // 16-bit storage: words [n_il][n_xl][ns] (q[t] | q[t+1] << 16) and one scale per trace
+    DevBuf words, scales;
     // adjoint: rows of each job (fold of duplicated output rows), image upload, job images
     std::vector<int> fold_map, fold_off;
     DevBuf d_fold_map, d_fold_off, img_in, fold;
@@ -169,6 +239,8 @@ namespace {
 FwdParams volume_params(psm_ctx* c) {
     FwdParams P{};
     P.pairs = c->pairs.as<float2>();
+    P.words = c->words.as<uint32_t>();
+    P.scales = c->scales.as<float>();
     P.vrms = c->vrms.as<float>();
     P.image = c->image.as<float>();
     P.jobs = c->d_jobs.as<Job>();
@@ -183,7 +255,7 @@ FwdParams volume_params(psm_ctx* c) {
     P.n_ox = c->g.n_ox;
     P.xoff = -c->g.pad_xl;
     P.max_inl = max_inline_window(c->jobs_all);
-    P.stage_cap = stage_cap(c->ns);
+    P.stage_cap = stage_cap(c->ns, c->store);
     fill_consts(P, c->g.dt, c->g.d_il, c->g.d_xl, c->g.tan2_theta);
     return P;
 }
@@ -233,6 +305,8 @@ int psm_destroy(psm_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->data.release();
     c->pairs.release();
+    c->words.release();
+    c->scales.release();
     c->vrms.release();
     c->image.release();
     c->d_jobs.release();
@@ -264,13 +338,16 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
         g->pad_il < 0 || g->pad_xl < 0 || g->m_il < 0 || !(g->dt > 0.0f) ||
         !(g->d_il > 0.0f) || !(g->d_xl > 0.0f) || !(g->tan2_theta >= 0.0f))
         return c->st.fail(PSM_ERR_ARG, "invalid geometry");
-    if (g->precision != PSM_F32)
-        return c->st.fail(PSM_ERR_UNSUPPORTED, "only PSM_F32 storage is built");
+    if (g->precision != PSM_F32 && g->precision != PSM_BF16 && g->precision != PSM_F16)
+        return c->st.fail(PSM_ERR_ARG, "precision must be PSM_F32, PSM_BF16 or PSM_F16");
+    const int store = store_of(g->precision);
     const int ns = trace_stride(g->n_t);
     // inline window of any output inline <= 2 (m_il + pad_il) + 1 (+ the inline table) and one
     // whole trace per ring stage must fit the CTA's shared memory
     const int64_t win = std::min<int64_t>(g->n_il, 2 * (int64_t(g->m_il) + g->pad_il) + 1);
-    if (psm::smem_layout(static_cast<int>(win), stage_cap(ns)).total > kMaxDynSmem)
+    if (psm::smem_layout(static_cast<int>(win), stage_cap(ns), 8).total > kMaxDynSmem ||
+        psm::smem_layout(static_cast<int>(win), stage_cap(ns, store), psm::store_bytes(store))
+                .total > kMaxDynSmem)
         return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t / aperture too large for the staging ring");
     std::vector<int> center(g->n_oi);
     for (int o = 0; o < g->n_oi; ++o) {
@@ -280,6 +357,7 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
     }
     c->g = *g;
     c->ns = ns;
+    c->store = store;
     c->jobs.clear();
     c->jobs_all.clear();
     c->copies.clear();
@@ -306,6 +384,10 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
     PSM_CUDA_TRY(c->st, c->data.ensure(n_tr * ns * sizeof(float)));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->data.p, 0, n_tr * ns * sizeof(float), c->stream));
     PSM_CUDA_TRY(c->st, c->pairs.ensure(n_tr * ns * sizeof(float2)));
+    if (store != psm::kStoreF32) {
+        PSM_CUDA_TRY(c->st, c->words.ensure(n_tr * ns * sizeof(uint32_t)));
+        PSM_CUDA_TRY(c->st, c->scales.ensure(n_tr * sizeof(float)));
+    }
     PSM_CUDA_TRY(c->st, c->vrms.ensure(n_tr * g->n_t * sizeof(float)));
     PSM_CUDA_TRY(c->st, c->image.ensure(static_cast<size_t>(g->n_oi) * g->n_ox * g->n_t *
                                         sizeof(float)));
@@ -359,8 +441,12 @@ int psm_set_traces(psm_ctx* c, const float* data) {
     PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.p, c->ns * sizeof(float), data,
                                           c->g.n_t * sizeof(float), c->g.n_t * sizeof(float),
                                           n_tr, cudaMemcpyHostToDevice, c->stream));
-    PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>(), c->pairs.as<float2>(), n_tr, c->ns,
-                                    c->stream));
+    if (c->store == psm::kStoreF32)
+        PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>(), c->pairs.as<float2>(), n_tr, c->ns,
+                                        c->stream));
+    else
+        PSM_CUDA_TRY(c->st, quantize(c->data.as<float>(), c->words.as<uint32_t>(),
+                                     c->scales.as<float>(), n_tr, c->ns, c->store, c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     c->have_traces = true;
     return PSM_OK;
@@ -386,7 +472,8 @@ int psm_forward_async(psm_ctx* c) {
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
     FwdParams P = volume_params(c);
     PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
-                                   c->g.amp_correction != 0, c->variant, c->stream));
+                                   c->g.amp_correction != 0, c->variant, c->stream, c->store,
+                                   c->g.compensated != 0));
     // padded output inlines repeat the migrated edge inline (main.cpp:268-285)
     const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
     for (const auto& cp : c->copies)
@@ -405,7 +492,7 @@ int psm_set_variant(psm_ctx* c, int variant) {
 
 int psm_get_variant(psm_ctx* c, int* variant) {
     if (!c || !variant) return PSM_ERR_ARG;
-    *variant = c->variant == PSM_FWD_DEFAULT ? kDefaultVariant : c->variant;
+    *variant = effective_variant(c->variant, c->store, c->g.compensated != 0);
     return PSM_OK;
 }
 
@@ -421,6 +508,7 @@ int psm_autotune(psm_ctx* c, float* ms, int* best) {
     float pick_ms = 3.0e38f;
     int rc = PSM_OK;
     for (int v = 1; v < PSM_FWD_N_VARIANTS && rc == PSM_OK; ++v) {
+        if (effective_variant(v, c->store, c->g.compensated != 0) != v) continue;  // same kernel
         c->variant = v;
         float t = 0.0f;
         if ((rc = psm_forward_async(c)) != PSM_OK) break;  // warm (first launch, attribute)
@@ -535,8 +623,10 @@ int forward_dev(psm_ctx* c, const float* d_vec, float* d_img) {
     PSM_CUDA_TRY(c->st, build_pairs(d_vec, c->pairs.as<float2>(), n_tr, c->ns, c->stream));
     FwdParams P = volume_params(c);
     P.image = d_img;
+    P.stage_cap = stage_cap(c->ns);  // the operator pair of CG is the fp32 one
     PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
-                                   c->g.amp_correction != 0, c->variant, c->stream));
+                                   c->g.amp_correction != 0, c->variant, c->stream,
+                                   psm::kStoreF32, c->g.compensated != 0));
     const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
     for (const auto& cp : c->copies)
         PSM_CUDA_TRY(c->st, cudaMemcpyAsync(d_img + cp.first * row, d_img + cp.second * row,
@@ -846,7 +936,8 @@ extern "C" int psm_forward_noalloc(const psm_geom* g, const int32_t* out_center,
     if (g->n_il <= 0 || g->n_xl <= 0 || g->n_t <= 0 || g->n_oi <= 0 || g->n_ox <= 0 ||
         g->pad_il < 0 || g->pad_xl < 0 || g->m_il < 0 || !(g->dt > 0.0f) ||
         !(g->d_il > 0.0f) || !(g->d_xl > 0.0f) || !(g->tan2_theta >= 0.0f) ||
-        g->precision != PSM_F32 || (reinterpret_cast<uintptr_t>(d_pairs) & 15u))
+        g->precision != PSM_F32 || g->compensated != 0 ||
+        (reinterpret_cast<uintptr_t>(d_pairs) & 15u))
         return PSM_ERR_ARG;
     if (g->n_oi > kNoallocMaxRows || g->n_il > kNoallocMaxInl || g->n_t > kNoallocMaxT)
         return PSM_ERR_UNSUPPORTED;

@@ -28,6 +28,8 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace psm {
@@ -40,8 +42,19 @@ constexpr int kMaxG = 32;       // traces per ring stage
 constexpr int kStageCapMin = 6144;          // samples (8 B each) per ring stage, at least
 constexpr unsigned kWaitLimit = 1u << 26;   // bounded mbarrier polls
 
+// Trace storage in HBM: fp32 pairs (d[t], d[t+1] - d[t]) (8 B a sample), or 16-bit words
+// (q[t] | q[t+1] << 16) of bf16 / fp16 values d / scale with one fp32 scale per trace.
+constexpr int kStoreF32 = 0;
+constexpr int kStoreBF16 = 1;
+constexpr int kStoreF16 = 2;
+__host__ __device__ constexpr int store_bytes(int store) { return store == kStoreF32 ? 8 : 4; }
+
 constexpr int PSM_DEV_ERR_TIMEOUT = 1;
-constexpr int PSM_DEV_ERR_WINDOW = 2;  // debug-bounds build only
+constexpr int PSM_DEV_ERR_WINDOW = 2;  // debug-bounds build (PSM_DEBUG_BOUNDS) only
+
+// Shared memory kept free after the staging ring: a read a few samples past the last staged
+// window stays inside the CTA's allocation.
+constexpr unsigned kSmemGuard = 128;
 
 // One output inline of a launch.
 struct Job {
@@ -54,7 +67,10 @@ struct Job {
 
 struct FwdParams {
     const float2* pairs;  // [n_ci][n_cx][ns] (d[t], d[t+1]-d[t]); rows 16 B aligned
-    const float* vrms;    // [n_vrow][n_vx][n_t] Vrms of the output points
+    const uint32_t* words;  // [n_ci][n_cx][ns] 16-bit storage: q[t] | q[t+1] << 16
+    const float* scales;    // [n_ci][n_cx] 16-bit storage: d = q * scale
+    const float* vrms;    // Vrms of the output points: (vrow, x, t) at vrow vs_row + x vs_x + t
+    long long vs_row, vs_x;  // element strides ([n_vrow][n_vx][n_t]; 0 broadcasts one trace)
     float* image;         // [rows][n_ox][n_t]
     const Job* jobs;
     const int* il_pos;    // [n_ci] inline positions
@@ -65,7 +81,7 @@ struct FwdParams {
     int n_ox;             // output crosslines per row
     int xoff;             // cube / Vrms crossline of output x is x + xoff
     int max_inl;          // largest i1 - i0 over the jobs (inline-table capacity)
-    int stage_cap;        // samples per ring stage
+    int stage_cap;        // samples per ring stage (of store_bytes each)
     float inv_dt, idt2, d_il, d_xl, inv_dxl, tan2, tanth;
     float ntm1f;          // n_t - 1
     float ntm1m;          // largest float below n_t - 1
@@ -77,6 +93,8 @@ struct StageMeta {
     int4 m[kMaxG];    // crossline, dx^2 (bits), window base (smem bytes, see consumers),
                       // window start as float (bits)
     float shi[kMaxG]; // largest s that stays inside the window
+    float sc[kMaxG];  // trace scale (16-bit storage)
+    float wend[kMaxG];  // window end as float (read by the debug-bounds build)
 };
 
 struct TileStats {
@@ -89,7 +107,7 @@ struct SmemLayout {
     unsigned full, empty, meta, stats, inl_klo, inl_pre, inl_dx2, stage, total;
 };
 
-__host__ __device__ inline SmemLayout smem_layout(int max_inl, int cap) {
+__host__ __device__ inline SmemLayout smem_layout(int max_inl, int cap, int elem_bytes = 8) {
     SmemLayout L;
     unsigned o = 0;
     L.full = o;
@@ -107,8 +125,8 @@ __host__ __device__ inline SmemLayout smem_layout(int max_inl, int cap) {
     L.inl_dx2 = o;
     o += 4 * max_inl;
     L.stage = o = (o + 127) & ~127u;
-    o += 8u * cap * kStages;
-    L.total = o;
+    o += static_cast<unsigned>(elem_bytes) * cap * kStages;
+    L.total = o + kSmemGuard;
     return L;
 }
 
@@ -224,6 +242,11 @@ __device__ __forceinline__ float warp_min(float v) {
 
 // ----------------------------------------------------------------------------- point setup
 
+// Vrms trace of output point (vrow, xv).
+__device__ __forceinline__ const float* vrms_trace(const FwdParams& P, int vrow, int xv) {
+    return P.vrms + vrow * P.vs_row + xv * P.vs_x;
+}
+
 // Per output sample constants in the reference's FP32 order (migration_kernel.cpp:115-144).
 // Division and products are pinned to round-to-nearest so the masks see the same numbers
 // as the reference build; that build (GCC, -ffp-contract=fast) fuses v*v + 1e-10.
@@ -297,6 +320,37 @@ __global__ void pair_kernel(const float* __restrict__ src, float2* __restrict__ 
     }
 }
 
+// 16-bit storage of rows of ns fp32 samples (zero beyond n_t): one warp per trace.
+// scale = max |d| over the trace (1 for an all-zero trace), q[t] = RNE(d[t] / scale) as
+// bf16 or fp16, words[t] = bits(q[t]) | bits(q[t+1]) << 16 with q[ns] = 0.
+template <int STORE>
+__device__ __forceinline__ uint32_t q16(float x) {
+    if (STORE == kStoreBF16) return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+    return __half_as_ushort(__float2half_rn(x));
+}
+
+template <int STORE>
+__global__ void quantize_kernel(const float* __restrict__ src, uint32_t* __restrict__ words,
+                                float* __restrict__ scales, size_t n_rows, int ns) {
+    const int lane = threadIdx.x & 31;
+    const size_t warps = static_cast<size_t>(gridDim.x) * (blockDim.x >> 5);
+    for (size_t r = blockIdx.x * static_cast<size_t>(blockDim.x >> 5) + (threadIdx.x >> 5);
+         r < n_rows; r += warps) {
+        const float* row = src + r * ns;
+        float m = 0.0f;
+        for (int t = lane; t < ns; t += 32) m = fmaxf(m, fabsf(row[t]));
+        m = warp_max(m);
+        const float scale = m > 0.0f ? m : 1.0f;
+        if (lane == 0) scales[r] = scale;
+        uint32_t* out = words + r * ns;
+        for (int t = lane; t < ns; t += 32) {
+            const uint32_t a = q16<STORE>(__fdiv_rn(row[t], scale));
+            const uint32_t b = t + 1 < ns ? q16<STORE>(__fdiv_rn(row[t + 1], scale)) : 0u;
+            out[t] = a | (b << 16);
+        }
+    }
+}
+
 // ----------------------------------------------------------------------------- forward
 
 // Producer: lo of every passing term of the tile on trace (dx2, kc) lies in [*lolo, *lohi]
@@ -326,22 +380,51 @@ __device__ __forceinline__ bool trace_bounds(const FwdParams& P, const TileStats
     return *lolo_out <= *lohi_out;
 }
 
-// Pair window of trace (dx2, kc) for the forward kernel: pairs [ws, we) with ws and we even
-// (16-byte TMA granularity for 8-byte samples) cover lo in [lolo, lohi]; size 0 when the
-// trace has no passing term.
+// Sample window of trace (dx2, kc) for the forward kernel: elements [ws, we) with ws and we
+// multiples of 16 / store_bytes (the TMA granularity) cover lo in [lolo, lohi + 1] (element
+// lo holds both interpolation operands; the extra element lets a passing term whose fast
+// s rounds up across lohi + 1 read staged data without a clamp); size 0 when the trace has
+// no passing term.  we <= ns: lohi + 2 <= n_t and ns is n_t rounded up to 8.
+template <int STORE>
 __device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats& S, int xa,
                                              int xb, float dx2, int kc, int* ws_out,
                                              int* size_out, float* shi_out) {
+    constexpr int A = 16 / store_bytes(STORE);
     *ws_out = 0;
     *size_out = 0;
     *shi_out = 0.0f;
     int lolo, lohi;
     if (!trace_bounds(P, S, xa, xb, dx2, kc, &lolo, &lohi)) return;
-    const int ws = lolo & ~1;
-    const int we = (lohi + 2) & ~1;  // pairs [ws, we) cover lo in [lolo, lohi]
+    const int ws = lolo & ~(A - 1);
+    const int we = (lohi + 1 + A) & ~(A - 1);  // elements [ws, we) cover [lolo, lohi + 1]
     *ws_out = ws;
     *size_out = we - ws;
     *shi_out = fminf(P.ntm1m, __uint_as_float(__float_as_uint(static_cast<float>(we)) - 1u));
+}
+
+// Staged window of one trace as the consumers see it.
+struct Win {
+    float wsf;  // first staged sample (float)
+    float shi;  // largest s whose element is staged, and below n_t - 1
+    float wef;  // end of the window (float): the debug-bounds build checks s < wef
+    int* err;
+};
+
+// s of a term, kept inside the staged window.  With MASK (some lane of the group may fail the
+// masks) s is clamped: a failing term's s can lie anywhere.  Without MASK every term of the
+// group passes both masks, and trace_window's bounds (two samples of slack, one extra
+// element) put floor(s) inside [ws, we): no clamp is needed.  The debug-bounds build checks
+// that claim and records PSM_DEV_ERR_WINDOW instead of reading outside the window.
+template <bool MASK>
+__device__ __forceinline__ float window_s(float s, const Win& w) {
+    if (MASK) return fminf(fmaxf(s, w.wsf), w.shi);
+#ifdef PSM_DEBUG_BOUNDS
+    if (!(s >= w.wsf && s < w.wef)) {
+        atomicOr(w.err, PSM_DEV_ERR_WINDOW);
+        return fminf(fmaxf(s, w.wsf), w.shi);
+    }
+#endif
+    return s;
 }
 
 // One pair of blocks (j, j+1) = (2 pr, 2 pr + 1) for one staged trace.
@@ -350,11 +433,11 @@ __device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats
 // One term of block-pair component (scalar FP32 arithmetic).
 template <bool AMP, bool MASK>
 __device__ __forceinline__ void term_one(const unsigned char* sbase, float r2, uint32_t base2,
-                                         float wsf, float shi, float T2, float F4, float BB,
+                                         const Win& w, float T2, float F4, float BB,
                                          float& ACC) {
     const float t2 = __fmaf_rn(F4, r2, T2);                  // (t / dt)^2
     const float q = rsqrtf(t2);                              // dt / t
-    const float s = fminf(fmaxf(t2 * q, wsf), shi);          // t / dt inside the window
+    const float s = window_s<MASK>(t2 * q, w);               // t / dt inside the window
     const float mm = __fadd_rd(s, 8388608.0f);               // 2^23 + floor(s)
     const float fr = s - (mm - 8388608.0f);                  // frac
     const float2 p =
@@ -369,18 +452,18 @@ __device__ __forceinline__ void term_one(const unsigned char* sbase, float r2, u
 
 template <bool AMP, bool MASK, bool PACKED>
 __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, uint32_t base2,
-                                          float wsf, float shi, const float2& T2,
+                                          const Win& w, const float2& T2,
                                           const float2& F4, const float2& BB, float2& ACC) {
     if (!PACKED) {
-        term_one<AMP, MASK>(sbase, r2, base2, wsf, shi, T2.x, F4.x, BB.x, ACC.x);
-        term_one<AMP, MASK>(sbase, r2, base2, wsf, shi, T2.y, F4.y, BB.y, ACC.y);
+        term_one<AMP, MASK>(sbase, r2, base2, w, T2.x, F4.x, BB.x, ACC.x);
+        term_one<AMP, MASK>(sbase, r2, base2, w, T2.y, F4.y, BB.y, ACC.y);
         return;
     }
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
     const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
     float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
-    s.x = fminf(fmaxf(s.x, wsf), shi);                       // inside the staged window
-    s.y = fminf(fmaxf(s.y, wsf), shi);
+    s.x = window_s<MASK>(s.x, w);                            // inside the staged window
+    s.y = window_s<MASK>(s.y, w);
     const float2 M = make_float2(8388608.0f, 8388608.0f);
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
@@ -400,18 +483,74 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
         ACC = add2(ACC, make_float2(v0, v1));
 }
 
+// Both samples of a 16-bit storage word as fp32 (exact conversions).
+template <int STORE>
+__device__ __forceinline__ float2 unpack16(uint32_t w) {
+    if (STORE == kStoreBF16)
+        return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+    return make_float2(__half2float(__ushort_as_half(static_cast<unsigned short>(w & 0xffffu))),
+                       __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16))));
+}
+
+// Block pair of one staged trace in 16-bit storage.  Sample n of the staged window sits at
+// byte base2 + (bits(2^23 + n) << 2); the interpolation takes the difference of the two
+// stored samples in fp32 (b - a, as the reference) and the trace scale joins the weight.
+template <bool AMP, bool MASK, int STORE>
+__device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2, uint32_t base2,
+                                            const Win& w, float sc, const float2& T2,
+                                            const float2& F4, const float2& BB, float2& ACC) {
+    const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
+    const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
+    float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
+    s.x = window_s<MASK>(s.x, w);                            // inside the staged window
+    s.y = window_s<MASK>(s.y, w);
+    const float2 M = make_float2(8388608.0f, 8388608.0f);
+    const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
+    const float2 fr = sub2(s, sub2(mm, M));                  // frac
+    const uint32_t w0 =
+        *reinterpret_cast<const uint32_t*>(sbase + (base2 + (__float_as_uint(mm.x) << 2)));
+    const uint32_t w1 =
+        *reinterpret_cast<const uint32_t*>(sbase + (base2 + (__float_as_uint(mm.y) << 2)));
+    const float2 p0 = unpack16<STORE>(w0), p1 = unpack16<STORE>(w1);
+    const float2 a = make_float2(p0.x, p1.x);
+    float2 v = fma2(fr, sub2(make_float2(p0.y, p1.y), a), a);  // simdInterpolate
+    if (MASK) {
+        v.x = r2 <= BB.x ? v.x : 0.0f;
+        v.y = r2 <= BB.y ? v.y : 0.0f;
+    }
+    if (AMP)
+        ACC = fma2(v, mul2(make_float2(q0, q1), make_float2(sc, sc)), ACC);
+    else
+        ACC = fma2(v, make_float2(sc, sc), ACC);
+}
+
 // Kernel variants: PACKED selects f32x2 or scalar FP32 arithmetic for a block pair; GB is
 // the number of 32-sample blocks behind one warp-uniform skip test (2 or 4); J the number
-// of 32-sample blocks per lane (the tile covers 32 J output samples).
-template <bool AMP, bool PACKED, int GB, int J>
-__global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
+// of 32-sample blocks per lane (the tile covers 32 J output samples).  STORE is the trace
+// storage (kStoreF32 pairs, or 16-bit words with a per-trace scale; 16-bit storage always
+// uses the packed arithmetic).  KAHAN adds compensated summation: each ring stage (at most
+// kMaxG traces) is summed into a fresh partial, and the partials are added to the
+// accumulator with Kahan's compensation, so the long sum over the aperture carries no
+// growing rounding error.
+//
+// fwd_tile computes one tile (output row job, crosslines [x0, x0 + kTX), samples
+// [T0, T0 + 32 J)) with all 9 warps of the CTA.  The ring's mbarriers are initialised once
+// per CTA (ring_init); it counts the ring stages the CTA has used so far, so consecutive tiles
+// of a persistent CTA continue the ring's phases (every stage, the end-of-stream marker
+// included, is released by the consumers).  Returns false when a bounded wait expired.
+template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN>
+__device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job& job, int x0, int T0,
+                                         unsigned char* smem_raw, const SmemLayout& L,
+                                         uint32_t& it) {
     static_assert(GB == 2 || GB == 4, "skip groups of 2 or 4 blocks");
     static_assert(J % GB == 0, "whole skip groups per lane");
+    static_assert(STORE == kStoreF32 || PACKED, "16-bit storage uses packed arithmetic");
     constexpr int NG = J / GB;   // skip groups per lane
     constexpr int PG = GB / 2;   // block pairs per group
     constexpr int TT = 32 * J;   // output samples per tile
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    const SmemLayout L = smem_layout(P.max_inl, P.stage_cap);
+    constexpr int EB = store_bytes(STORE);
+    // bits(2^23) << log2(EB), modulo 2^32 (see the producer)
+    constexpr uint32_t MAGIC = EB == 8 ? 0x58000000u : 0x2C000000u;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + L.full);
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem_raw + L.empty);
     StageMeta* meta = reinterpret_cast<StageMeta*>(smem_raw + L.meta);
@@ -420,20 +559,18 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const Job job = P.jobs[blockIdx.z];
-    const int x0 = blockIdx.x * kTX;
-    const int T0 = blockIdx.y * TT;
 
     // ---- consumers: per-sample constants (J / 2 register pairs) and tile statistics
     float2 T2[J / 2], F4[J / 2], BB[J / 2], ACC[J / 2];
+    float2 PART[J / 2], CMP[J / 2];  // KAHAN: stage partials and compensation
+    float2(&SUM)[J / 2] = KAHAN ? PART : ACC;
     float gmax[NG], gmin[NG];
     float warpmax = -1.0f;
     const int x = x0 + warp - 1;
     const int xv = x + P.xoff;
     if (warp > 0) {
         const bool xvalid = x < P.n_ox && xv >= 0 && xv < P.n_vx;
-        const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
-                                    (xvalid ? xv : 0)) * P.n_t;
+        const float* vp = vrms_trace(P, job.vrow, xvalid ? xv : 0);
         float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
         float bj[J];
 #pragma unroll
@@ -468,7 +605,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
             }
         }
 #pragma unroll
-        for (int p = 0; p < J / 2; ++p) ACC[p] = make_float2(0.0f, 0.0f);
+        for (int p = 0; p < J / 2; ++p) {
+            ACC[p] = make_float2(0.0f, 0.0f);
+            CMP[p] = make_float2(0.0f, 0.0f);
+        }
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
             float mx = bj[GB * g], mn = bj[GB * g];
@@ -496,12 +636,6 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
             s.any = bmax >= 0.0f;
             wstats[warp - 1] = s;
         }
-    } else if (lane == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kTX);
-        }
-        fence_barrier_init();
     }
     __syncthreads();
 
@@ -561,13 +695,12 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
             if (lane == 0) inl_pre[n_inl] = total;
             __syncwarp();
         }
-        uint32_t it = 0;
         bool alive = true;
         int f = 0;
         while (f < total && alive) {
             const int idx = f + lane;
             int ws = 0, size = 0, kc = 0, row = 0;
-            float dx2 = 0.0f, shi = 0.0f;
+            float dx2 = 0.0f, shi = 0.0f, sc = 1.0f;
             if (idx < total) {
                 // buffer inline of flat trace idx: the last n with inl_pre[n] <= idx
                 int lo = 0, hi = n_inl - 1;
@@ -581,7 +714,9 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
                 kc = inl_klo[lo] + (idx - inl_pre[lo]);
                 dx2 = inl_dx2[lo];
                 row = job.i0 + lo;
-                trace_window(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
+                trace_window<STORE>(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
+                if (STORE != kStoreF32 && size > 0)
+                    sc = __ldg(P.scales + static_cast<size_t>(row) * P.n_cx + kc);
             }
             // inclusive prefix sum of window sizes; take the lanes that fit one stage
             int cum = size;
@@ -606,75 +741,126 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
                 StageMeta& m = meta[stage];
                 const int tot = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
                 const uint32_t dst_rel =
-                    L.stage + (static_cast<uint32_t>(stage) * P.stage_cap + (cum - size)) * 8u;
+                    L.stage + (static_cast<uint32_t>(stage) * P.stage_cap + (cum - size)) * EB;
                 const uint32_t dst = stage0 + (dst_rel - L.stage);
                 if (take && size > 0) {
                     const int slot = __popc(nzmask & ((1u << lane) - 1u));
                     // consumers find sample n of the window at byte
-                    // base2 + (bits(2^23 + n) << 3) from the shared-memory base (32-bit
-                    // wrap-around): base2 = dst_rel - 8 ws - (0x4B000000 << 3)
+                    // base2 + (bits(2^23 + n) << log2(EB)) from the shared-memory base (32-bit
+                    // wrap-around): base2 = dst_rel - EB ws - (0x4B000000 << log2(EB))
                     m.m[slot] = make_int4(kc, __float_as_int(dx2),
-                                          static_cast<int>(dst_rel - 8u * ws - 0x58000000u),
+                                          static_cast<int>(dst_rel - EB * ws - MAGIC),
                                           __float_as_int(static_cast<float>(ws)));
                     m.shi[slot] = shi;
+                    m.sc[slot] = sc;
+                    m.wend[slot] = static_cast<float>(ws + size);
                 }
                 if (lane == 0) m.count = n;
                 __threadfence_block();
                 __syncwarp();
-                if (lane == 0) mbar_arrive_expect_tx(&full[stage], static_cast<uint32_t>(tot) * 8u);
+                if (lane == 0)
+                    mbar_arrive_expect_tx(&full[stage], static_cast<uint32_t>(tot) * EB);
                 __syncwarp();
-                if (take && size > 0)
-                    tma_load_1d(dst,
-                                P.pairs + (static_cast<size_t>(row) * P.n_cx + kc) * P.ns + ws,
-                                static_cast<uint32_t>(size) * 8u, &full[stage]);
+                if (take && size > 0) {
+                    const size_t off = (static_cast<size_t>(row) * P.n_cx + kc) * P.ns + ws;
+                    const void* src = STORE == kStoreF32
+                                          ? static_cast<const void*>(P.pairs + off)
+                                          : static_cast<const void*>(P.words + off);
+                    tma_load_1d(dst, src, static_cast<uint32_t>(size) * EB, &full[stage]);
+                }
                 ++it;
             }
             f += consumed;
         }
         // end-of-stream marker
-        if (alive && lane == 0) {
-            const int stage = it % kStages;
-            const uint32_t par = ((it / kStages) & 1u) ^ 1u;
-            if (mbar_wait(&empty[stage], par, P.err)) {
-                meta[stage].count = -1;
-                __threadfence_block();
-                mbar_arrive(&full[stage]);
+        if (alive) {
+            int ok = 1;
+            if (lane == 0) {
+                const int stage = it % kStages;
+                const uint32_t par = ((it / kStages) & 1u) ^ 1u;
+                ok = mbar_wait(&empty[stage], par, P.err);
+                if (ok) {
+                    meta[stage].count = -1;
+                    __threadfence_block();
+                    mbar_arrive(&full[stage]);
+                }
             }
+            alive = __shfl_sync(0xffffffffu, ok, 0) != 0;
+            ++it;
         }
-        return;
+        return alive;
     }
 
     // -------------------------------------------------------------------- consumers
-    uint32_t it = 0;
+    bool alive = true;
     while (true) {
         const int stage = it % kStages;
         const uint32_t par = (it / kStages) & 1u;
-        if (!mbar_wait(&full[stage], par, P.err)) break;
+        if (!mbar_wait(&full[stage], par, P.err)) {
+            alive = false;
+            break;
+        }
         const StageMeta& m = meta[stage];
         const int cnt = m.count;
-        if (cnt < 0) break;
+        if (cnt < 0) {  // end of stream: release the marker's stage too
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[stage]);
+            ++it;
+            break;
+        }
+        if (KAHAN) {
+#pragma unroll
+            for (int p = 0; p < J / 2; ++p) PART[p] = make_float2(0.0f, 0.0f);
+        }
         for (int g = 0; g < cnt; ++g) {
             const int4 md = m.m[g];
             const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
             if (r2 > warpmax) continue;
             const uint32_t base2 = static_cast<uint32_t>(md.z);
-            const float wsf = __int_as_float(md.w);
-            const float shi = m.shi[g];
+            Win w;
+            w.wsf = __int_as_float(md.w);
+            w.shi = m.shi[g];
+#ifdef PSM_DEBUG_BOUNDS
+            w.wef = m.wend[g];
+#else
+            w.wef = 0.0f;
+#endif
+            w.err = P.err;
+            const float sc = STORE == kStoreF32 ? 1.0f : m.sc[g];
 #pragma unroll
             for (int gr = 0; gr < NG; ++gr) {
                 if (r2 <= gmax[gr]) {
                     if (r2 <= gmin[gr]) {  // every lane of the group passes
 #pragma unroll
-                        for (int p = PG * gr; p < PG * (gr + 1); ++p)
-                            term_pair<AMP, false, PACKED>(smem_raw, r2, base2, wsf, shi, T2[p],
-                                                          F4[p], BB[p], ACC[p]);
+                        for (int p = PG * gr; p < PG * (gr + 1); ++p) {
+                            if (STORE == kStoreF32)
+                                term_pair<AMP, false, PACKED>(smem_raw, r2, base2, w,
+                                                              T2[p], F4[p], BB[p], SUM[p]);
+                            else
+                                term_pair16<AMP, false, STORE>(smem_raw, r2, base2, w,
+                                                               sc, T2[p], F4[p], BB[p], SUM[p]);
+                        }
                     } else {
 #pragma unroll
-                        for (int p = PG * gr; p < PG * (gr + 1); ++p)
-                            term_pair<AMP, true, PACKED>(smem_raw, r2, base2, wsf, shi, T2[p],
-                                                         F4[p], BB[p], ACC[p]);
+                        for (int p = PG * gr; p < PG * (gr + 1); ++p) {
+                            if (STORE == kStoreF32)
+                                term_pair<AMP, true, PACKED>(smem_raw, r2, base2, w,
+                                                             T2[p], F4[p], BB[p], SUM[p]);
+                            else
+                                term_pair16<AMP, true, STORE>(smem_raw, r2, base2, w,
+                                                              sc, T2[p], F4[p], BB[p], SUM[p]);
+                        }
                     }
                 }
+            }
+        }
+        if (KAHAN) {  // ACC += PART, compensated
+#pragma unroll
+            for (int p = 0; p < J / 2; ++p) {
+                const float2 y = sub2(PART[p], CMP[p]);
+                const float2 t = add2(ACC[p], y);
+                CMP[p] = sub2(sub2(t, ACC[p]), y);
+                ACC[p] = t;
             }
         }
         __syncwarp();
@@ -685,8 +871,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
     // ---- write the tile: weight 1/(t v^2) = (dt/t) * inv_dt / v^2 applied per output sample
     if (x < P.n_ox) {
         const bool xvalid = xv >= 0 && xv < P.n_vx;
-        const float* vp = P.vrms + (static_cast<size_t>(job.vrow) * P.n_vx +
-                                    (xvalid ? xv : 0)) * P.n_t;
+        const float* vp = vrms_trace(P, job.vrow, xvalid ? xv : 0);
         float* op = P.image + (static_cast<size_t>(job.row) * P.n_ox + x) * P.n_t;
 #pragma unroll
         for (int j = 0; j < J; ++j) {
@@ -707,6 +892,69 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
             }
         }
     }
+    return alive;
+}
+
+// The ring's mbarriers: full (one producer arrival + the TMA bytes), empty (kTX consumers).
+__device__ __forceinline__ void ring_init(unsigned char* smem_raw, const SmemLayout& L) {
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + L.full);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem_raw + L.empty);
+    for (int s = 0; s < kStages; ++s) {
+        mbar_init(&full[s], 1);
+        mbar_init(&empty[s], kTX);
+    }
+    fence_barrier_init();
+}
+
+// One tile per CTA: grid (crossline tiles, time tiles, jobs).
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false>
+__global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
+    if (threadIdx.x == 0) ring_init(smem_raw, L);  // ordered by the tile's first barrier
+    uint32_t it = 0;
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
+                                               blockIdx.y * 32 * J, smem_raw, L, it);
+}
+
+// One tile of a batched launch: problem, job of that problem, first crossline and sample.
+struct BatchItem {
+    int prob, job, x0, T0;
+};
+
+// Persistent batched launch: each CTA takes tiles from the shared list in order (an atomic
+// counter) until the list is exhausted, with the ring kept across tiles.  Problems (velocity
+// panels, sub-volumes) each have their own FwdParams; the CTA copies the current problem's
+// parameters to shared memory.  max_inl and stage_cap are the largest over the problems.
+// A device error (bounded wait expired) stops every CTA at its next tile.
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false>
+__global__ void __launch_bounds__(32 * (kTX + 1), 2)
+    fwd_batch_kernel(const FwdParams* __restrict__ probs, const BatchItem* __restrict__ items,
+                     int n_items, int* next, const int* err, int max_inl, int stage_cap) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ FwdParams s_P;
+    __shared__ Job s_job;
+    __shared__ BatchItem s_item;
+    const SmemLayout L = smem_layout(max_inl, stage_cap, store_bytes(STORE));
+    if (threadIdx.x == 0) ring_init(smem_raw, L);
+    uint32_t it = 0;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const int k = *reinterpret_cast<const volatile int*>(err) ? n_items
+                                                                      : atomicAdd(next, 1);
+            s_item = k < n_items ? items[k] : BatchItem{-1, 0, 0, 0};
+            if (k < n_items) {
+                s_P = probs[s_item.prob];
+                s_job = s_P.jobs[s_item.job];
+            }
+        }
+        __syncthreads();
+        if (s_item.prob < 0) break;
+        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(s_P, s_job, s_item.x0,
+                                                                  s_item.T0, smem_raw, L, it);
+        // barrier: the tile's tables, statistics and s_P are reused next
+        if (__syncthreads_or(!ok)) break;
+    }
 }
 
 // ----------------------------------------------------------------------------- term count
@@ -723,7 +971,7 @@ __global__ void count_kernel(const FwdParams P, unsigned long long* out) {
     unsigned long long local = 0;
     for (int t = threadIdx.x; t < P.n_t; t += blockDim.x) {
         if (xv < 0 || xv >= P.n_vx) break;
-        const float v = P.vrms[(static_cast<size_t>(job.vrow) * P.n_vx + xv) * P.n_t + t];
+        const float v = vrms_trace(P, job.vrow, xv)[t];
         const PointConst pc = point_const(v, P.t0[t], P.tan2);
         const float B = pass_bound(pc, P.inv_dt, P.ntm1f);
         if (B < 0.0f) continue;

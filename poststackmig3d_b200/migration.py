@@ -108,6 +108,7 @@ class Geometry:
     out_center: np.ndarray
     amp: bool = True
     precision: str = "f32"
+    compensated: bool = False
 
     @property
     def dt(self) -> float:
@@ -122,7 +123,7 @@ class Geometry:
         return PsmGeom(self.n_il, self.n_xl, self.n_t, self.pad_il, self.pad_xl, self.n_oi,
                        self.n_ox, self.m_il, int(bool(self.amp)), PRECISIONS[self.precision],
                        np.float32(self.dt_seconds), self.d_il, self.d_xl, self.tan2,
-                       self.dt_seconds)
+                       self.dt_seconds, int(bool(self.compensated)))
 
 
 def plan_geometry(n_il: int, n_xl: int, n_t: int, dt_seconds: float, d_il: float,
