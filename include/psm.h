@@ -108,6 +108,90 @@ int psm_get_image(psm_ctx *ctx, float *image);
 /* Raw CUDA stream of the ctx (a cudaStream_t). */
 int psm_stream(psm_ctx *ctx, void **stream);
 
+/* ---- Slabs of output inlines: out-of-core streaming and sharding across GPUs.  No
+ * counterpart in the reference, which re-reads each output inline's input window from the
+ * file (prepareInputBufferWithPadding, src/migration_kernel.cpp:385-468).  A slab is output
+ * inlines [o0, o1) and the input inlines [i0, i1) their buffers read (each output inline o
+ * reads [c - m_il - pad_il, c + m_il + 1 + pad_il) around its centre c, clamped to the cube,
+ * migration_kernel.cpp:404-409); migrating the slab on its own gives exactly those rows of the
+ * whole image. */
+typedef struct {
+    int32_t o0, o1; /* output inlines */
+    int32_t i0, i1; /* input inlines */
+} psm_slab;
+
+/* Device bytes a slab of n_in input inlines and n_out output inlines holds while it is
+ * migrated (traces as uploaded and in the storage the kernel stages, Vrms, image). */
+int64_t psm_slab_bytes(const psm_geom *g, int32_t n_in, int32_t n_out);
+/* Split the output inlines into consecutive slabs of at most max_device_bytes each
+ * (max_device_bytes <= 0: one slab).  slabs[max_slabs]; *n_slabs the count.
+ * PSM_ERR_UNSUPPORTED when one output inline alone exceeds the budget, PSM_ERR_ARG when
+ * max_slabs is too small. */
+int psm_plan_slabs(const psm_geom *g, const int32_t *out_center, int64_t max_device_bytes,
+                   psm_slab *slabs, int32_t max_slabs, int32_t *n_slabs);
+/* Split the output inlines into n_parts consecutive slabs of about equal work, the work of
+ * output inline o being weight[o] (NULL: 1 each), for sharding over n_parts GPUs. */
+int psm_split_slabs(const psm_geom *g, const int32_t *out_center, const double *weight,
+                    int32_t n_parts, psm_slab *slabs);
+/* Geometry of a slab on its own: n_il = i1 - i0, n_oi = o1 - o0, and local_center[n_oi] the
+ * slab's output centres relative to i0 (for psm_set_geometry with traces and Vrms from input
+ * inline i0 on). */
+int psm_slab_geometry(const psm_geom *g, const int32_t *out_center, const psm_slab *slab,
+                      psm_geom *local, int32_t *local_center);
+/* Forward migration of a cube held in host memory, streamed through the ctx in slabs of at
+ * most max_device_bytes: traces and vrms [n_il][n_xl][n_t] (host) in, image
+ * [n_oi][n_ox][n_t] (host) out.  For cubes larger than the GPU's memory. */
+int psm_forward_streamed(psm_ctx *ctx, const psm_geom *g, const int32_t *out_center,
+                         const float *traces, const float *vrms, float *image,
+                         int64_t max_device_bytes);
+
+/* ---- Vrms assembled on the GPU into the ctx's Vrms cube [n_il][n_xl][n_t] (what
+ * psm_set_vrms uploads), at sample times t * dt_seconds.  No counterpart in the reference,
+ * whose providers loop on the CPU (src/velocity_reader.cpp); the operations and their order
+ * are the host providers' (include/psm_host.h), so the cube is the same bit for bit.
+ *   psm_set_vrms_table: the text-table provider (:264-370): points (il, xl, time in s, v);
+ *     every point blends into every sample with weight 1 / (1 + dist), an exact hit returns its
+ *     v, a non-positive result the smallest v.
+ *   psm_set_vrms_grid: the SEG-Y provider (:33-261) on its dense grid [g_nil][g_nxl][g_nt]
+ *     (sorted labels, missing traces zero, sample interval g_dt): points on grid labels copy
+ *     or interpolate their trace in time, others blend the 2x2 label neighbours.
+ * il_labels[n_il], xl_labels[n_xl] are the cube's labels. */
+int psm_set_vrms_table(psm_ctx *ctx, const int32_t *p_il, const int32_t *p_xl,
+                       const double *p_time, const float *p_v, int32_t n_points,
+                       const int32_t *il_labels, const int32_t *xl_labels);
+int psm_set_vrms_grid(psm_ctx *ctx, const float *grid, const int32_t *g_il, int32_t g_nil,
+                      const int32_t *g_xl, int32_t g_nxl, int32_t g_nt, double g_dt,
+                      const int32_t *il_labels, const int32_t *xl_labels);
+/* The ctx's Vrms cube (host out). */
+int psm_get_vrms(psm_ctx *ctx, float *vrms);
+
+/* ---- SEG-Y trace codec on the GPU.  No counterpart in the reference, which decodes and
+ * encodes every trace on the CPU (readTraceData, src/segy_utils.cpp:272-318, with ibmToIeee
+ * :243-254; writeTrace :598-648 with ieeeToIbm :257-270); the bytes are the same.
+ *
+ * psm_set_traces_segy uploads n_records trace records exactly as they follow the file's 3600
+ * header bytes (a 240-byte header and n_t big-endian samples each; format 1 IBM, anything
+ * else IEEE) and decodes them on the GPU into the resident cube: record r fills cube trace
+ * position[r] (il_index * n_xl + xl_index), or nothing when position[r] is -1 (zero labels,
+ * or a duplicate (IL, XL) that a later record overrides, segy_utils.cpp:164-204).  Traces no
+ * record fills are zero.  The upload runs in 32 MB chunks on a second stream, overlapped with
+ * the decode when the records are in pinned memory.  The records stay on the device as the
+ * header sources of psm_get_image_segy. */
+int psm_set_traces_segy(psm_ctx *ctx, const void *records, int64_t n_records, int32_t format,
+                        const int32_t *position);
+/* Encodes the ctx image as n_oi * n_ox output records (240 + 4 n_t bytes each, host `out`):
+ * output trace r = o * n_ox + x copies the header of uploaded record source[r], or, for
+ * source[r] = -1, gets a zero header with INLINE_3D@188 = il_label[o] and CROSSLINE_3D@192 =
+ * xl_label[x] (segy_utils.cpp:605-620, main.cpp:393-413); samples big-endian, format 1 IBM
+ * (the reference's truncating ieeeToIbm; +-inf -> sign|0x7FFFFFFF, NaN -> 0x40000000, where
+ * the reference never terminates) or IEEE. */
+int psm_get_image_segy(psm_ctx *ctx, void *out, int32_t format, const int32_t *source,
+                       const int32_t *il_label, const int32_t *xl_label);
+/* The resident fp32 cube [n_il][n_xl][n_t] as uploaded or decoded (host out). */
+int psm_get_traces(psm_ctx *ctx, float *data);
+/* Overwrite the ctx image [n_oi][n_ox][n_t] from the host (e.g. to encode a given image). */
+int psm_set_image(psm_ctx *ctx, const float *image);
+
 /* Adjoint of psm_forward (demigration / spray, M^T): data[n_il][n_xl][n_t] (host, output)
  * from image[n_oi][n_ox][n_t] (host).  Every term of the forward is spread back with its
  * transposed interpolation weights (1 - frac, frac) and the same amplitude weight, so
@@ -150,6 +234,69 @@ int psm_autotune(psm_ctx *ctx, float *ms, int *best);
 int psm_count_terms(psm_ctx *ctx, int64_t *n_terms);
 /* The same count per output inline: per_row[n_oi]. */
 int psm_count_terms_rows(psm_ctx *ctx, int64_t *per_row);
+
+/* ---- Batched migration: several problems (velocity-scan panels over one cube, uneven
+ * sub-volumes with their own Vrms) in ONE persistent launch, replayed as a CUDA graph.  No
+ * counterpart in the reference, which migrates one cube with one velocity field per run
+ * (src/main.cpp:291-361); each problem is exactly that run's operator. */
+typedef enum {
+    PSM_VRMS_CUBE = 0,     /* vrms [n_il][n_xl][n_t], as psm_set_vrms */
+    PSM_VRMS_TRACE = 1,    /* vrms [n_t]: one Vrms(t) for every output point */
+    PSM_VRMS_CONSTANT = 2  /* velocity for every point and sample (a scan panel) */
+} psm_vrms_kind;
+
+typedef struct {
+    psm_geom geom;             /* amp_correction, precision and compensated equal for all */
+    const int32_t *out_center; /* [geom.n_oi] or NULL, as psm_set_geometry */
+    const float *traces;       /* host [n_il][n_xl][n_t]; problems that pass the same pointer
+                                  and grid share one device copy */
+    const float *vrms;         /* see vrms_kind; unused for PSM_VRMS_CONSTANT */
+    int32_t vrms_kind;
+    float velocity;            /* PSM_VRMS_CONSTANT */
+} psm_problem;
+
+typedef struct psm_batch psm_batch;
+
+typedef enum {
+    PSM_BATCH_PERSISTENT = 0,  /* one persistent launch over every problem's tiles */
+    PSM_BATCH_PER_PROBLEM = 1  /* one grid launch per problem */
+} psm_batch_mode;
+
+/* At most 192 problems (PSM_ERR_UNSUPPORTED beyond): their parameters travel as one kernel
+ * argument.  Uploads every problem (the host arrays are read again by psm_batch_reload, so
+ * they must stay valid while the batch lives) and builds the tile lists (psm_tile_order).
+ * Images stay on the device. */
+int psm_batch_create(psm_ctx *ctx, const psm_problem *problems, int n_problems,
+                     psm_batch **out);
+int psm_batch_destroy(psm_batch *batch);
+int psm_batch_reload(psm_batch *batch); /* re-upload traces and Vrms from the host arrays */
+/* Either mode runs as one CUDA graph (captured on the first run of a variant / order /
+ * mode, then replayed). */
+int psm_batch_set_mode(psm_batch *batch, int mode);
+int psm_batch_get_mode(psm_batch *batch, int *mode);
+int psm_batch_set_variant(psm_batch *batch, int variant);
+int psm_batch_get_variant(psm_batch *batch, int *variant);
+
+/* Order in which the persistent CTAs take the tiles. */
+typedef enum {
+    PSM_ORDER_DEPTH_FIRST = 0, /* deepest time tiles first, problems interleaved per tile */
+    PSM_ORDER_PROBLEM = 1      /* problem after problem, each in grid order */
+} psm_tile_order;
+int psm_batch_set_order(psm_batch *batch, int order);
+int psm_batch_get_order(psm_batch *batch, int *order);
+/* Times one run per distinct kernel variant on each of three schedules (persistent
+ * depth-first, persistent problem order, one launch per problem) and keeps the fastest
+ * variant, order and mode; ms[3 * PSM_FWD_N_VARIANTS] (may be NULL) receives the times at
+ * [schedule * PSM_FWD_N_VARIANTS + variant], 0 for variants not run. */
+int psm_batch_autotune(psm_batch *batch, float *ms, int *best, int *best_order,
+                       int *best_mode);
+int psm_batch_run_async(psm_batch *batch); /* on the context's stream */
+int psm_batch_synchronize(psm_batch *batch);
+int psm_batch_run(psm_batch *batch);       /* run_async + synchronize */
+int psm_batch_image_device(psm_batch *batch, int problem, float **dev_image);
+int psm_batch_get_image(psm_batch *batch, int problem, float *image);
+/* Terms over all problems (psm_count_terms of each). */
+int psm_batch_count_terms(psm_batch *batch, int64_t *n_terms);
 
 /* Per-inline drop-in for MigrationKernel::kirchhoffKernel3DWithPadding
  * (include/migration_kernel.h:16-31, src/migration_kernel.cpp:17-383): the same arguments,

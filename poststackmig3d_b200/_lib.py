@@ -27,6 +27,13 @@ class PsmGeom(ctypes.Structure):
                 ("compensated", ctypes.c_int32)]
 
 
+class PsmProblem(ctypes.Structure):
+    """Mirror of psm_problem (include/psm.h)."""
+    _fields_ = [("geom", PsmGeom), ("out_center", ctypes.c_void_p),
+                ("traces", ctypes.c_void_p), ("vrms", ctypes.c_void_p),
+                ("vrms_kind", ctypes.c_int32), ("velocity", ctypes.c_float)]
+
+
 class PsmError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS.get(code, code)}: {msg}")
@@ -54,11 +61,38 @@ _CUDA_SYMBOLS = [
     ("psm_stream", ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     ("psm_count_terms", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     ("psm_count_terms_rows", ctypes.c_int, [_P, _P]),
+    ("psm_set_vrms_table", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int32, _P, _P]),
+    ("psm_set_vrms_grid", ctypes.c_int, [_P, _P, _P, ctypes.c_int32, _P, ctypes.c_int32,
+                                         ctypes.c_int32, ctypes.c_double, _P, _P]),
+    ("psm_get_vrms", ctypes.c_int, [_P, _P]),
+    ("psm_set_traces_segy", ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int32, _P]),
+    ("psm_get_image_segy", ctypes.c_int, [_P, _P, ctypes.c_int32, _P, _P, _P]),
+    ("psm_get_traces", ctypes.c_int, [_P, _P]),
+    ("psm_set_image", ctypes.c_int, [_P, _P]),
     ("psm_adjoint", ctypes.c_int, [_P, _P, _P]),
     ("psm_lsm_cg", ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P]),
     ("psm_set_variant", ctypes.c_int, [_P, ctypes.c_int]),
     ("psm_get_variant", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     ("psm_autotune", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_int)]),
+    ("psm_batch_create", ctypes.c_int, [_P, ctypes.POINTER(PsmProblem), ctypes.c_int,
+                                        ctypes.POINTER(_P)]),
+    ("psm_batch_destroy", ctypes.c_int, [_P]),
+    ("psm_batch_reload", ctypes.c_int, [_P]),
+    ("psm_batch_set_mode", ctypes.c_int, [_P, ctypes.c_int]),
+    ("psm_batch_set_variant", ctypes.c_int, [_P, ctypes.c_int]),
+    ("psm_batch_get_variant", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    ("psm_batch_set_order", ctypes.c_int, [_P, ctypes.c_int]),
+    ("psm_batch_get_order", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    ("psm_batch_autotune", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
+    ("psm_batch_get_mode", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    ("psm_batch_run_async", ctypes.c_int, [_P]),
+    ("psm_batch_synchronize", ctypes.c_int, [_P]),
+    ("psm_batch_run", ctypes.c_int, [_P]),
+    ("psm_batch_image_device", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),
+    ("psm_batch_get_image", ctypes.c_int, [_P, ctypes.c_int, _P]),
+    ("psm_batch_count_terms", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     ("psm_kirchhoff_inline", ctypes.c_int,
      [_P, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, _P, _P, ctypes.c_size_t, _P, _P,
       ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _P, ctypes.c_float, ctypes.c_float,

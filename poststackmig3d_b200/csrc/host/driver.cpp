@@ -169,19 +169,15 @@ void run(const Config& cfg, bool verbose, Plan* plan_only) {
         return;
     }
 
-    // dense cubes on the real grid: traces and the output points' Vrms (main.cpp:296-321)
     Timer t_io;
-    std::vector<float> data(n_il * n_xl * n_t), vrms(n_il * n_xl * n_t);
-    in.read_cube(data.data());
-    for (size_t i = 0; i < n_il; ++i)
-        prov->velocity_iline(il[i], xl, n_t, dt, vrms.data() + i * n_xl * n_t);
     const double s_io = t_io.s();
 
     if (verbose) out << "\n[5/6] Migrating on the GPU..." << std::endl;
     Timer t_gpu;
     psm_ctx* ctx = nullptr;
     cuda_check(psm_create(&ctx, cfg.device), nullptr, "psm_create");
-    std::vector<float> image(out_il.size() * out_xl.size() * n_t);
+    const size_t n_out = out_il.size() * out_xl.size();
+    std::vector<unsigned char> records(n_out * (240 + 4 * n_t));
     try {
         psm_geom g{};
         g.n_il = static_cast<int32_t>(n_il);
@@ -201,9 +197,24 @@ void run(const Config& cfg, bool verbose, Plan* plan_only) {
         g.tan2_theta = tan2;
         g.dt_seconds = dt;
         cuda_check(psm_set_geometry(ctx, &g, centers.data()), ctx, "psm_set_geometry");
-        cuda_check(psm_set_traces(ctx, data.data()), ctx, "psm_set_traces");
-        cuda_check(psm_set_vrms(ctx, vrms.data()), ctx, "psm_set_vrms");
-        cuda_check(psm_forward(ctx, image.data()), ctx, "psm_forward");
+        const std::vector<int32_t> pos = in.record_positions();
+        cuda_check(psm_set_traces_segy(ctx, in.trace_records(), in.num_traces(), in.format(),
+                                       pos.data()),
+                   ctx, "psm_set_traces_segy");
+        // the output points' Vrms on the real grid (main.cpp:296-321): assembled on the GPU
+        // for the table and SEG-Y providers, filled on the host for a constant
+        if (!prov->assemble_on_gpu(ctx, il, xl)) {
+            std::vector<float> vrms(n_il * n_xl * n_t);
+            for (size_t i = 0; i < n_il; ++i)
+                prov->velocity_iline(il[i], xl, n_t, dt, vrms.data() + i * n_xl * n_t);
+            cuda_check(psm_set_vrms(ctx, vrms.data()), ctx, "psm_set_vrms");
+        }
+        cuda_check(psm_forward_async(ctx), ctx, "psm_forward_async");
+        // output records encoded on the GPU (segy_utils.cpp:398-487, :598-648)
+        const std::vector<int32_t> src = output_sources(in, out_il, out_xl, il_pad);
+        cuda_check(psm_get_image_segy(ctx, records.data(), in.format(), src.data(),
+                                      out_il.data(), out_xl.data()),
+                   ctx, "psm_get_image_segy");
     } catch (...) {
         psm_destroy(ctx);
         throw;
@@ -213,7 +224,7 @@ void run(const Config& cfg, bool verbose, Plan* plan_only) {
 
     if (verbose) out << "\n[6/6] Writing output file..." << std::endl;
     Timer t_w;
-    write_output(cfg.output_data, in, out_il, out_xl, il_pad, image.data());
+    write_output_records(cfg.output_data, in, records.data(), n_out);
     if (verbose) {
         out << "Output dimensions: IL=" << out_il.size() << ", XL=" << out_xl.size()
             << "\n\nMigration complete!\n\nTotal time: " << std::fixed << std::setprecision(2)

@@ -12,6 +12,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include "psm.h"
+
 namespace psmhost {
 
 struct Error : std::runtime_error {
@@ -82,6 +84,11 @@ public:
     void read_trace_at(int32_t il, int32_t xl, float* out) const;
     // Dense cube [n_il][n_xl][ns] on the sorted labels, missing traces zero.
     void read_cube(float* cube) const;
+    // The trace records as they follow the 3600 header bytes (num_traces() records of
+    // 240 + 4 num_samples() bytes), and for each the cube trace il_index * n_xl + xl_index it
+    // fills, or -1 (zero labels, or a duplicate that a later record overrides).
+    const unsigned char* trace_records() const { return trace_header(0); }
+    std::vector<int32_t> record_positions() const;
 
 private:
     std::string path_;
@@ -100,6 +107,13 @@ private:
 void write_output(const std::string& path, const Segy& in,
                   const std::vector<int32_t>& out_il, const std::vector<int32_t>& out_xl,
                   const std::vector<char>& il_is_padding, const float* image);
+// The same file from output records already encoded (psm_get_image_segy): the header
+// sources of those rules, and the file written around the records.
+std::vector<int32_t> output_sources(const Segy& in, const std::vector<int32_t>& out_il,
+                                    const std::vector<int32_t>& out_xl,
+                                    const std::vector<char>& il_is_padding);
+void write_output_records(const std::string& path, const Segy& in, const unsigned char* records,
+                          size_t n_records);
 
 // ----------------------------------------------------------------------------- velocity
 
@@ -110,6 +124,13 @@ public:
     // default: per-sample velocity() (velocity_reader.cpp:424-441)
     virtual void velocity_iline(int32_t il, const std::vector<int32_t>& xl, size_t n_t,
                                 double dt, float* out /*[n_xl][n_t]*/);
+    // Assemble the Vrms cube of ctx's geometry on the GPU (psm_set_vrms_table /
+    // psm_set_vrms_grid) with the same arithmetic; false when the provider has no GPU path
+    // (the caller then uploads velocity_iline's cube).
+    virtual bool assemble_on_gpu(psm_ctx*, const std::vector<int32_t>& /*il*/,
+                                 const std::vector<int32_t>& /*xl*/) {
+        return false;
+    }
 };
 
 std::unique_ptr<VelocityProvider> make_velocity_provider(const std::string& param);

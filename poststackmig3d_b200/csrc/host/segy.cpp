@@ -122,17 +122,60 @@ void Segy::read_cube(float* cube) const {
         read_trace_at(il_[t / n_xl], xl_[t % n_xl], cube + t * ns_);
 }
 
+std::vector<int32_t> Segy::record_positions() const {
+    std::vector<int32_t> pos(static_cast<size_t>(n_traces_), -1);
+    const int64_t n_xl = static_cast<int64_t>(xl_.size());
+    for (const auto& kv : lookup_) {
+        const int64_t a = std::lower_bound(il_.begin(), il_.end(), kv.first.first) - il_.begin();
+        const int64_t b = std::lower_bound(xl_.begin(), xl_.end(), kv.first.second) - xl_.begin();
+        pos[static_cast<size_t>(kv.second)] = static_cast<int32_t>(a * n_xl + b);
+    }
+    return pos;
+}
+
+std::vector<int32_t> output_sources(const Segy& in, const std::vector<int32_t>& out_il,
+                                    const std::vector<int32_t>& out_xl,
+                                    const std::vector<char>& il_is_padding) {
+    std::vector<int32_t> src(out_il.size() * out_xl.size(), -1);
+    for (size_t o = 0; o < out_il.size(); ++o) {
+        if (il_is_padding[o]) continue;
+        for (size_t x = 0; x < out_xl.size(); ++x) {
+            auto it = in.lookup().find({out_il[o], out_xl[x]});
+            if (it != in.lookup().end())
+                src[o * out_xl.size() + x] = static_cast<int32_t>(it->second);
+        }
+    }
+    return src;
+}
+
+static std::vector<unsigned char> output_file_header(const Segy& in) {
+    std::vector<unsigned char> head(kTextHeader + kBinaryHeader);
+    std::memcpy(head.data(), in.text_header(), kTextHeader);
+    std::memcpy(head.data() + kTextHeader, in.binary_header(), kBinaryHeader);
+    put_be16(head.data() + kTextHeader + 20, static_cast<uint16_t>(in.num_samples()));
+    put_be16(head.data() + kTextHeader + 24, static_cast<uint16_t>(in.format()));
+    return head;
+}
+
+void write_output_records(const std::string& path, const Segy& in, const unsigned char* records,
+                          size_t n_records) {
+    const std::vector<unsigned char> head = output_file_header(in);
+    const size_t bytes = n_records * (kTraceHeader + 4 * static_cast<size_t>(in.num_samples()));
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw Error("Cannot create output SEGY file: " + path);
+    bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();
+    ok = ok && std::fwrite(records, 1, bytes, f) == bytes;
+    if (std::fclose(f) != 0) ok = false;
+    if (!ok) throw Error("Failed to write output SEGY file: " + path);
+}
+
 void write_output(const std::string& path, const Segy& in, const std::vector<int32_t>& out_il,
                   const std::vector<int32_t>& out_xl, const std::vector<char>& il_is_padding,
                   const float* image) {
     const size_t ns = static_cast<size_t>(in.num_samples());
     const size_t tr = kTraceHeader + 4 * ns;
     const size_t n_oi = out_il.size(), n_ox = out_xl.size();
-    std::vector<unsigned char> head(kTextHeader + kBinaryHeader);
-    std::memcpy(head.data(), in.text_header(), kTextHeader);
-    std::memcpy(head.data() + kTextHeader, in.binary_header(), kBinaryHeader);
-    put_be16(head.data() + kTextHeader + 20, static_cast<uint16_t>(ns));
-    put_be16(head.data() + kTextHeader + 24, static_cast<uint16_t>(in.format()));
+    const std::vector<unsigned char> head = output_file_header(in);
     FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) throw Error("Cannot create output SEGY file: " + path);
     bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();

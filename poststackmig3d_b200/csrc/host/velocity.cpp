@@ -58,6 +58,20 @@ public:
         return blend(il, xl, time);
     }
 
+    bool assemble_on_gpu(psm_ctx* ctx, const std::vector<int32_t>& il,
+                         const std::vector<int32_t>& xl) override {
+        const auto& gi = f_.il_labels();
+        const auto& gx = f_.xl_labels();
+        std::vector<float> grid(gi.size() * gx.size() * n_t_);
+        f_.read_cube(grid.data());
+        const int rc = psm_set_vrms_grid(ctx, grid.data(), gi.data(), static_cast<int32_t>(gi.size()),
+                                         gx.data(), static_cast<int32_t>(gx.size()),
+                                         static_cast<int32_t>(n_t_), dt_, il.data(), xl.data());
+        if (rc != PSM_OK)
+            throw Error(std::string("psm_set_vrms_grid failed: ") + psm_last_error(ctx));
+        return true;
+    }
+
     void velocity_iline(int32_t il, const std::vector<int32_t>& xl, size_t n_t, double dt,
                         float* out) override {  // :203-261
         std::fill(out, out + xl.size() * n_t, 0.0f);
@@ -186,6 +200,24 @@ public:
         float r = sw > 0 ? sv / sw : vmin_;
         if (r <= 0) r = vmin_;
         return r;
+    }
+
+    bool assemble_on_gpu(psm_ctx* ctx, const std::vector<int32_t>& il,
+                         const std::vector<int32_t>& xl) override {
+        std::vector<int32_t> p_il, p_xl;
+        std::vector<double> p_t;
+        std::vector<float> p_v;
+        for (const auto& p : pts_) {
+            p_il.push_back(p.il);
+            p_xl.push_back(p.xl);
+            p_t.push_back(p.time);
+            p_v.push_back(p.v);
+        }
+        const int rc = psm_set_vrms_table(ctx, p_il.data(), p_xl.data(), p_t.data(), p_v.data(),
+                                          static_cast<int32_t>(pts_.size()), il.data(), xl.data());
+        if (rc != PSM_OK)
+            throw Error(std::string("psm_set_vrms_table failed: ") + psm_last_error(ctx));
+        return true;
     }
 
 private:

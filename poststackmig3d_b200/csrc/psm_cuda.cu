@@ -14,6 +14,8 @@
 #include "psm.h"
 #include "psm_adjoint.cuh"
 #include "psm_kernels.cuh"
+#include "psm_segy.cuh"
+#include "psm_vrms.cuh"
 
 namespace {
 
@@ -88,43 +90,6 @@ size_t fwd_smem(const FwdParams& P, int store = psm::kStoreF32) {
     return b <= kMaxDynSmem ? b : 0;
 }
 
-template <bool AMP, bool PACKED, int GB, int J, int STORE = psm::kStoreF32, bool KAHAN = false>
-cudaError_t launch_fwd_v(const FwdParams& P, int n_jobs, size_t smem, cudaStream_t s) {
-    constexpr int TT = 32 * J;
-    auto* kern = psm::fwd_kernel<AMP, PACKED, GB, J, STORE, KAHAN>;
-    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + TT - 1) / TT, n_jobs);
-    dim3 block(32 * (psm::kTX + 1));
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    kern<<<grid, block, smem, s>>>(P);
-    return cudaGetLastError();
-}
-
-// 16-bit storage and compensated summation: the packed kernel with skip groups of 4, with
-// 8 or 16 blocks a lane (8 only with compensation: its partial and compensation registers
-// leave no room for 16).
-template <bool AMP, int STORE, bool KAHAN>
-cudaError_t launch_fwd_sk(const FwdParams& P, int n_jobs, bool j16, size_t smem,
-                          cudaStream_t s) {
-    if (!KAHAN && j16) return launch_fwd_v<AMP, true, 4, 16, STORE, false>(P, n_jobs, smem, s);
-    return launch_fwd_v<AMP, true, 4, 8, STORE, KAHAN>(P, n_jobs, smem, s);
-}
-
-template <bool AMP>
-cudaError_t launch_fwd_amp(const FwdParams& P, int n_jobs, int variant, size_t smem,
-                           cudaStream_t s) {
-    switch (variant) {
-        case PSM_FWD_SCALAR_G2: return launch_fwd_v<AMP, false, 2, 8>(P, n_jobs, smem, s);
-        case PSM_FWD_SCALAR_G4: return launch_fwd_v<AMP, false, 4, 8>(P, n_jobs, smem, s);
-        case PSM_FWD_PACKED_G2: return launch_fwd_v<AMP, true, 2, 8>(P, n_jobs, smem, s);
-        case PSM_FWD_PACKED_G4: return launch_fwd_v<AMP, true, 4, 8>(P, n_jobs, smem, s);
-        case PSM_FWD_PACKED_G4_J16: return launch_fwd_v<AMP, true, 4, 16>(P, n_jobs, smem, s);
-        case PSM_FWD_SCALAR_G4_J16: return launch_fwd_v<AMP, false, 4, 16>(P, n_jobs, smem, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
 constexpr int kDefaultVariant = PSM_FWD_PACKED_G4;
 
 inline bool is_j16(int variant) {
@@ -132,31 +97,86 @@ inline bool is_j16(int variant) {
 }
 
 // The variant that actually runs: 16-bit storage runs the packed skip-4 kernel with the
-// variant's blocks per lane, compensated summation the packed skip-4 kernel with 8.
+// variant's blocks per lane, compensated summation the packed skip-4 kernel with 8 (its
+// partial and compensation registers leave no room for 16).
 inline int effective_variant(int variant, int store, bool kahan) {
     if (variant == PSM_FWD_DEFAULT) variant = kDefaultVariant;
     if (store == psm::kStoreF32 && !kahan) return variant;
     return !kahan && is_j16(variant) ? PSM_FWD_PACKED_G4_J16 : PSM_FWD_PACKED_G4;
 }
 
-template <bool AMP>
-cudaError_t launch_fwd_mode(const FwdParams& P, int n_jobs, int variant, int store, bool kahan,
-                            size_t smem, cudaStream_t s) {
+// One instantiation of the forward kernel templates.
+template <bool AMP_, bool PACKED_, int GB_, int J_, int STORE_, bool KAHAN_>
+struct KernelTag {
+    static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_;
+    static constexpr int GB = GB_, J = J_, STORE = STORE_;
+};
+
+// Calls f(KernelTag<...>{}) for the kernel that (amp, effective variant, store, kahan) names.
+template <bool AMP, class F>
+cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
+    using psm::kStoreBF16;
+    using psm::kStoreF16;
+    using psm::kStoreF32;
     const bool j16 = is_j16(variant);
     switch (store * 2 + (kahan ? 1 : 0)) {
-        case psm::kStoreF32 * 2: return launch_fwd_amp<AMP>(P, n_jobs, variant, smem, s);
-        case psm::kStoreF32 * 2 + 1:
-            return launch_fwd_sk<AMP, psm::kStoreF32, true>(P, n_jobs, j16, smem, s);
-        case psm::kStoreBF16 * 2:
-            return launch_fwd_sk<AMP, psm::kStoreBF16, false>(P, n_jobs, j16, smem, s);
-        case psm::kStoreBF16 * 2 + 1:
-            return launch_fwd_sk<AMP, psm::kStoreBF16, true>(P, n_jobs, j16, smem, s);
-        case psm::kStoreF16 * 2:
-            return launch_fwd_sk<AMP, psm::kStoreF16, false>(P, n_jobs, j16, smem, s);
-        case psm::kStoreF16 * 2 + 1:
-            return launch_fwd_sk<AMP, psm::kStoreF16, true>(P, n_jobs, j16, smem, s);
+        case kStoreF32 * 2:
+            switch (variant) {
+                case PSM_FWD_SCALAR_G2: return f(KernelTag<AMP, false, 2, 8, kStoreF32, false>{});
+                case PSM_FWD_SCALAR_G4: return f(KernelTag<AMP, false, 4, 8, kStoreF32, false>{});
+                case PSM_FWD_PACKED_G2: return f(KernelTag<AMP, true, 2, 8, kStoreF32, false>{});
+                case PSM_FWD_PACKED_G4: return f(KernelTag<AMP, true, 4, 8, kStoreF32, false>{});
+                case PSM_FWD_PACKED_G4_J16:
+                    return f(KernelTag<AMP, true, 4, 16, kStoreF32, false>{});
+                case PSM_FWD_SCALAR_G4_J16:
+                    return f(KernelTag<AMP, false, 4, 16, kStoreF32, false>{});
+                default: return cudaErrorInvalidValue;
+            }
+        case kStoreF32 * 2 + 1: return f(KernelTag<AMP, true, 4, 8, kStoreF32, true>{});
+        case kStoreBF16 * 2:
+            return j16 ? f(KernelTag<AMP, true, 4, 16, kStoreBF16, false>{})
+                       : f(KernelTag<AMP, true, 4, 8, kStoreBF16, false>{});
+        case kStoreBF16 * 2 + 1: return f(KernelTag<AMP, true, 4, 8, kStoreBF16, true>{});
+        case kStoreF16 * 2:
+            return j16 ? f(KernelTag<AMP, true, 4, 16, kStoreF16, false>{})
+                       : f(KernelTag<AMP, true, 4, 8, kStoreF16, false>{});
+        case kStoreF16 * 2 + 1: return f(KernelTag<AMP, true, 4, 8, kStoreF16, true>{});
         default: return cudaErrorInvalidValue;
     }
+}
+
+template <class F>
+cudaError_t with_kernel(bool amp, int variant, int store, bool kahan, F&& f) {
+    variant = effective_variant(variant, store, kahan);
+    return amp ? with_kernel_amp<true>(variant, store, kahan, f)
+               : with_kernel_amp<false>(variant, store, kahan, f);
+}
+
+// The grid kernel's shared-memory limit, set before a stream capture (the attribute belongs
+// to the kernel, so it must cover the largest launch of the capture).
+template <class K>
+cudaError_t prepare_grid(K, size_t smem) {
+    return cudaFuncSetAttribute(psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem));
+}
+
+template <class K>
+cudaError_t launch_grid(K, const FwdParams& P, int n_jobs, size_t smem, cudaStream_t s) {
+    constexpr int TT = 32 * K::J;
+    auto* kern = psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + TT - 1) / TT, n_jobs);
+    dim3 block(32 * (psm::kTX + 1));
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return e;
+    if (cap == cudaStreamCaptureStatusNone) {  // a capture was prepared by prepare_grid
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<grid, block, smem, s>>>(P);
+    return cudaGetLastError();
 }
 
 // Launch the forward kernel for n_jobs jobs (P.max_inl and P.stage_cap set; P.pairs for fp32
@@ -166,9 +186,8 @@ cudaError_t launch_fwd(const FwdParams& P, int n_jobs, bool amp, int variant, cu
     if (n_jobs <= 0 || P.n_ox <= 0 || P.n_t <= 0) return cudaSuccess;
     const size_t smem = fwd_smem(P, store);
     if (!smem) return cudaErrorInvalidValue;
-    variant = effective_variant(variant, store, kahan);
-    return amp ? launch_fwd_mode<true>(P, n_jobs, variant, store, kahan, smem, s)
-               : launch_fwd_mode<false>(P, n_jobs, variant, store, kahan, smem, s);
+    return with_kernel(amp, variant, store, kahan,
+                       [&](auto k) { return launch_grid(k, P, n_jobs, smem, s); });
 }
 
 // words[n_rows][ns] and scales[n_rows] from the fp32 rows (quantize_kernel, one warp a row).
@@ -206,6 +225,64 @@ void fill_consts(FwdParams& P, float dt, float d_il, float d_xl, float tan2) {
     P.vs_row = static_cast<long long>(P.n_vx) * P.n_t;
 }
 
+// Argument checks of a geometry: PSM_OK, or the status with *why set.
+int check_geometry(const psm_geom& g, std::string* why) {
+    if (g.n_il <= 0 || g.n_xl <= 0 || g.n_t <= 0 || g.n_oi <= 0 || g.n_ox <= 0 || g.pad_il < 0 ||
+        g.pad_xl < 0 || g.m_il < 0 || !(g.dt > 0.0f) || !(g.d_il > 0.0f) || !(g.d_xl > 0.0f) ||
+        !(g.tan2_theta >= 0.0f)) {
+        *why = "invalid geometry";
+        return PSM_ERR_ARG;
+    }
+    if (g.precision != PSM_F32 && g.precision != PSM_BF16 && g.precision != PSM_F16) {
+        *why = "precision must be PSM_F32, PSM_BF16 or PSM_F16";
+        return PSM_ERR_ARG;
+    }
+    const int store = store_of(g.precision);
+    const int ns = trace_stride(g.n_t);
+    // inline window of any output inline <= 2 (m_il + pad_il) + 1 (+ the inline table) and one
+    // whole trace per ring stage must fit the CTA's shared memory
+    const int64_t win = std::min<int64_t>(g.n_il, 2 * (int64_t(g.m_il) + g.pad_il) + 1);
+    if (psm::smem_layout(static_cast<int>(win), stage_cap(ns), 8).total > kMaxDynSmem ||
+        psm::smem_layout(static_cast<int>(win), stage_cap(ns, store), psm::store_bytes(store))
+                .total > kMaxDynSmem) {
+        *why = "n_t / aperture too large for the staging ring";
+        return PSM_ERR_UNSUPPORTED;
+    }
+    return PSM_OK;
+}
+
+// Jobs of a geometry: one per output inline (jobs_all, for term counts) and one per distinct
+// migrated inline (jobs), the repeated output rows as (row, row it copies).  Padded output
+// inlines migrate the nearest real inline (main.cpp:258-288); the buffer of real inline c is
+// inlines [c - m_il - pad_il, c + m_il + 1 + pad_il) clamped to the cube
+// (migration_kernel.cpp:404-409).  False when out_center names an inline outside the cube.
+bool plan_jobs(const psm_geom& g, const int32_t* out_center, std::vector<Job>& jobs,
+               std::vector<Job>& jobs_all, std::vector<std::pair<int, int>>& copies) {
+    jobs.clear();
+    jobs_all.clear();
+    copies.clear();
+    std::vector<int> first_row(g.n_il, -1);
+    for (int o = 0; o < g.n_oi; ++o) {
+        const int cc = out_center ? out_center[o] : std::min(std::max(o - g.pad_il, 0), g.n_il - 1);
+        if (cc < 0 || cc >= g.n_il) return false;
+        const int rs = std::max(0, cc - g.m_il), re = std::min(g.n_il, cc + g.m_il + 1);
+        Job j;
+        j.row = o;
+        j.vrow = cc;
+        j.pos = cc;
+        j.i0 = std::max(0, rs - g.pad_il);
+        j.i1 = std::min(g.n_il, re + g.pad_il);
+        jobs_all.push_back(j);
+        if (first_row[cc] < 0) {
+            first_row[cc] = o;
+            jobs.push_back(j);
+        } else {
+            copies.emplace_back(o, first_row[cc]);
+        }
+    }
+    return true;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------- context
@@ -232,6 +309,13 @@ struct psm_ctx {
     DevBuf d_fold_map, d_fold_off, img_in, fold;
     // least-squares migration vectors: data space [n_tr][ns], image space [n_oi][n_ox][n_t]
     DevBuf cg_d, cg_r, cg_q, cg_m, cg_s, cg_p, cg_sc, cg_hist;
+    // SEG-Y codec: the input trace records as uploaded, their cube positions, the output
+    // records and their header sources / labels; a copy stream overlaps upload and decode
+    DevBuf seg_rec, seg_pos, seg_out, seg_src, seg_il, seg_xl;
+    int64_t seg_n = 0;
+    int seg_rec_bytes = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copied = nullptr;
 };
 
 namespace {
@@ -316,8 +400,12 @@ int psm_destroy(psm_ctx* c) {
     c->err.release();
     c->count.release();
     for (DevBuf* b : {&c->d_fold_map, &c->d_fold_off, &c->img_in, &c->fold, &c->cg_d, &c->cg_r,
-                      &c->cg_q, &c->cg_m, &c->cg_s, &c->cg_p, &c->cg_sc, &c->cg_hist})
+                      &c->cg_q, &c->cg_m, &c->cg_s, &c->cg_p, &c->cg_sc, &c->cg_hist,
+                      &c->seg_rec, &c->seg_pos, &c->seg_out, &c->seg_src, &c->seg_il,
+                      &c->seg_xl})
         b->release();
+    if (c->copied) cudaEventDestroy(c->copied);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSM_OK;
@@ -334,52 +422,21 @@ int psm_stream(psm_ctx* c, void** s) {
 int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
     if (!c || !g) return PSM_ERR_ARG;
     cudaSetDevice(c->device);
-    if (g->n_il <= 0 || g->n_xl <= 0 || g->n_t <= 0 || g->n_oi <= 0 || g->n_ox <= 0 ||
-        g->pad_il < 0 || g->pad_xl < 0 || g->m_il < 0 || !(g->dt > 0.0f) ||
-        !(g->d_il > 0.0f) || !(g->d_xl > 0.0f) || !(g->tan2_theta >= 0.0f))
-        return c->st.fail(PSM_ERR_ARG, "invalid geometry");
-    if (g->precision != PSM_F32 && g->precision != PSM_BF16 && g->precision != PSM_F16)
-        return c->st.fail(PSM_ERR_ARG, "precision must be PSM_F32, PSM_BF16 or PSM_F16");
+    std::string why;
+    int rc = check_geometry(*g, &why);
+    if (rc) return c->st.fail(rc, why);
+    std::vector<Job> jobs, jobs_all;
+    std::vector<std::pair<int, int>> copies;
+    if (!plan_jobs(*g, out_center, jobs, jobs_all, copies))
+        return c->st.fail(PSM_ERR_ARG, "out_center out of range");
     const int store = store_of(g->precision);
     const int ns = trace_stride(g->n_t);
-    // inline window of any output inline <= 2 (m_il + pad_il) + 1 (+ the inline table) and one
-    // whole trace per ring stage must fit the CTA's shared memory
-    const int64_t win = std::min<int64_t>(g->n_il, 2 * (int64_t(g->m_il) + g->pad_il) + 1);
-    if (psm::smem_layout(static_cast<int>(win), stage_cap(ns), 8).total > kMaxDynSmem ||
-        psm::smem_layout(static_cast<int>(win), stage_cap(ns, store), psm::store_bytes(store))
-                .total > kMaxDynSmem)
-        return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t / aperture too large for the staging ring");
-    std::vector<int> center(g->n_oi);
-    for (int o = 0; o < g->n_oi; ++o) {
-        int cc = out_center ? out_center[o] : std::min(std::max(o - g->pad_il, 0), g->n_il - 1);
-        if (cc < 0 || cc >= g->n_il) return c->st.fail(PSM_ERR_ARG, "out_center out of range");
-        center[o] = cc;
-    }
     c->g = *g;
     c->ns = ns;
     c->store = store;
-    c->jobs.clear();
-    c->jobs_all.clear();
-    c->copies.clear();
-    std::vector<int> first_row(g->n_il, -1);
-    for (int o = 0; o < g->n_oi; ++o) {
-        const int cc = center[o];
-        // buffer inlines (migration_kernel.cpp:404-409)
-        const int rs = std::max(0, cc - g->m_il), re = std::min(g->n_il, cc + g->m_il + 1);
-        Job j;
-        j.row = o;
-        j.vrow = cc;
-        j.pos = cc;
-        j.i0 = std::max(0, rs - g->pad_il);
-        j.i1 = std::min(g->n_il, re + g->pad_il);
-        c->jobs_all.push_back(j);
-        if (first_row[cc] < 0) {
-            first_row[cc] = o;
-            c->jobs.push_back(j);
-        } else {
-            c->copies.emplace_back(o, first_row[cc]);
-        }
-    }
+    c->jobs.swap(jobs);
+    c->jobs_all.swap(jobs_all);
+    c->copies.swap(copies);
     const size_t n_tr = static_cast<size_t>(g->n_il) * g->n_xl;
     PSM_CUDA_TRY(c->st, c->data.ensure(n_tr * ns * sizeof(float)));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->data.p, 0, n_tr * ns * sizeof(float), c->stream));
@@ -449,6 +506,215 @@ int psm_set_traces(psm_ctx* c, const float* data) {
                                      c->scales.as<float>(), n_tr, c->ns, c->store, c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     c->have_traces = true;
+    return PSM_OK;
+}
+
+int psm_get_traces(psm_ctx* c, float* data) {
+    if (!c || !data) return PSM_ERR_ARG;
+    if (!c->have_traces) return c->st.fail(PSM_ERR_STATE, "no traces uploaded");
+    cudaSetDevice(c->device);
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(data, c->g.n_t * sizeof(float), c->data.p,
+                                          c->ns * sizeof(float), c->g.n_t * sizeof(float), n_tr,
+                                          cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    return PSM_OK;
+}
+
+int psm_set_traces_segy(psm_ctx* c, const void* records, int64_t n_records, int32_t format,
+                        const int32_t* position) {
+    if (!c || n_records < 0 || (n_records && (!records || !position))) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    const int64_t n_tr = static_cast<int64_t>(c->g.n_il) * c->g.n_xl;
+    {  // every record fills at most one cube trace, every cube trace at most once
+        std::vector<unsigned char> seen(static_cast<size_t>(n_tr), 0);
+        for (int64_t r = 0; r < n_records; ++r) {
+            const int32_t p = position[r];
+            if (p < -1 || p >= n_tr || (p >= 0 && seen[p]++))
+                return c->st.fail(PSM_ERR_ARG, "position " + std::to_string(r) +
+                                                   ": out of range or repeated");
+        }
+    }
+    const int rec_bytes = psm::kSegyTraceHeader + 4 * c->g.n_t;
+    cudaStream_t s = c->stream;
+    if (!c->copy_stream) {
+        PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        PSM_CUDA_TRY(c->st, cudaEventCreateWithFlags(&c->copied, cudaEventDisableTiming));
+    }
+    PSM_CUDA_TRY(c->st, c->seg_rec.ensure(static_cast<size_t>(n_records) * rec_bytes));
+    PSM_CUDA_TRY(c->st, c->seg_pos.ensure(static_cast<size_t>(n_records) * sizeof(int32_t)));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->data.p, 0, n_tr * c->ns * sizeof(float), s));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->seg_pos.p, position, n_records * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, s));
+    // chunks of about 32 MB: the copy of chunk k + 1 (copy stream) overlaps the decode of
+    // chunk k (ctx stream) when the records are in pinned memory
+    const int64_t per_chunk = std::max<int64_t>(1, (int64_t(32) << 20) / rec_bytes);
+    PSM_CUDA_TRY(c->st, cudaEventRecord(c->copied, s));  // the copy stream follows the memsets
+    PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, c->copied, 0));
+    for (int64_t r0 = 0; r0 < n_records; r0 += per_chunk) {
+        const int64_t n = std::min(per_chunk, n_records - r0);
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->seg_rec.as<unsigned char>() + r0 * rec_bytes,
+                                            static_cast<const unsigned char*>(records) +
+                                                r0 * rec_bytes,
+                                            static_cast<size_t>(n) * rec_bytes,
+                                            cudaMemcpyHostToDevice, c->copy_stream));
+        PSM_CUDA_TRY(c->st, cudaEventRecord(c->copied, c->copy_stream));
+        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(s, c->copied, 0));
+        const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((n + 7) / 8, 148 * 16));
+        psm::segy_decode_kernel<<<blocks, 256, 0, s>>>(
+            c->seg_rec.as<unsigned char>() + r0 * rec_bytes, n, rec_bytes, c->g.n_t, c->ns,
+            format, c->seg_pos.as<int32_t>() + r0, c->data.as<float>());
+        PSM_CUDA_TRY(c->st, cudaGetLastError());
+    }
+    if (c->store == psm::kStoreF32)
+        PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>(), c->pairs.as<float2>(),
+                                        static_cast<size_t>(n_tr), c->ns, s));
+    else
+        PSM_CUDA_TRY(c->st, quantize(c->data.as<float>(), c->words.as<uint32_t>(),
+                                     c->scales.as<float>(), static_cast<size_t>(n_tr), c->ns,
+                                     c->store, s));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
+    c->seg_n = n_records;
+    c->seg_rec_bytes = rec_bytes;
+    c->have_traces = true;
+    return PSM_OK;
+}
+
+int psm_set_image(psm_ctx* c, const float* image) {
+    if (!c || !image) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    const size_t n = static_cast<size_t>(c->g.n_oi) * c->g.n_ox * c->g.n_t;
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.p, image, n * sizeof(float),
+                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    return PSM_OK;
+}
+
+int psm_get_image_segy(psm_ctx* c, void* out, int32_t format, const int32_t* source,
+                       const int32_t* il_label, const int32_t* xl_label) {
+    if (!c || !out || !source || !il_label || !xl_label) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    const int64_t n_out = static_cast<int64_t>(c->g.n_oi) * c->g.n_ox;
+    for (int64_t r = 0; r < n_out; ++r)
+        if (source[r] < -1 || source[r] >= c->seg_n ||
+            (source[r] >= 0 && c->seg_rec_bytes != psm::kSegyTraceHeader + 4 * c->g.n_t))
+            return c->st.fail(PSM_ERR_ARG, "source " + std::to_string(r) +
+                                               ": no such uploaded record");
+    const int out_rec_bytes = psm::kSegyTraceHeader + 4 * c->g.n_t;
+    cudaStream_t s = c->stream;
+    PSM_CUDA_TRY(c->st, c->seg_out.ensure(static_cast<size_t>(n_out) * out_rec_bytes));
+    PSM_CUDA_TRY(c->st, c->seg_src.ensure(static_cast<size_t>(n_out) * sizeof(int32_t)));
+    PSM_CUDA_TRY(c->st, c->seg_il.ensure(c->g.n_oi * sizeof(int32_t)));
+    PSM_CUDA_TRY(c->st, c->seg_xl.ensure(c->g.n_ox * sizeof(int32_t)));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->seg_src.p, source, n_out * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, s));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->seg_il.p, il_label, c->g.n_oi * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, s));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->seg_xl.p, xl_label, c->g.n_ox * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, s));
+    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((n_out + 7) / 8, 148 * 16));
+    psm::segy_encode_kernel<<<blocks, 256, 0, s>>>(
+        c->image.as<float>(), n_out, c->g.n_ox, c->g.n_t, format, c->seg_src.as<int32_t>(),
+        c->seg_rec.as<unsigned char>(), c->seg_rec_bytes, c->seg_il.as<int32_t>(),
+        c->seg_xl.as<int32_t>(), c->seg_out.as<unsigned char>());
+    PSM_CUDA_TRY(c->st, cudaGetLastError());
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(out, c->seg_out.p,
+                                        static_cast<size_t>(n_out) * out_rec_bytes,
+                                        cudaMemcpyDeviceToHost, s));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
+    return read_device_error(c);
+}
+
+int psm_get_vrms(psm_ctx* c, float* vrms) {
+    if (!c || !vrms) return PSM_ERR_ARG;
+    if (!c->have_vrms) return c->st.fail(PSM_ERR_STATE, "no Vrms set");
+    cudaSetDevice(c->device);
+    const size_t n = static_cast<size_t>(c->g.n_il) * c->g.n_xl * c->g.n_t;
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(vrms, c->vrms.p, n * sizeof(float),
+                                        cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    return PSM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Upload n values to a temporary device buffer (freed by the caller's DevBuf).
+template <class T>
+cudaError_t upload(DevBuf& b, const T* host, size_t n, cudaStream_t s) {
+    cudaError_t e = b.ensure(std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess || !n) return e;
+    return cudaMemcpyAsync(b.p, host, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+inline unsigned vrms_blocks(size_t n) {
+    return static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 32)));
+}
+
+}  // namespace
+
+extern "C" {
+
+int psm_set_vrms_table(psm_ctx* c, const int32_t* p_il, const int32_t* p_xl,
+                       const double* p_time, const float* p_v, int32_t n_points,
+                       const int32_t* il_labels, const int32_t* xl_labels) {
+    if (!c || n_points <= 0 || !p_il || !p_xl || !p_time || !p_v || !il_labels || !xl_labels)
+        return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    float vmin = p_v[0];
+    for (int32_t i = 1; i < n_points; ++i) vmin = std::min(vmin, p_v[i]);
+    cudaStream_t s = c->stream;
+    DevBuf d_il, d_xl, d_t, d_v, d_lil, d_lxl;
+    PSM_CUDA_TRY(c->st, upload(d_il, p_il, n_points, s));
+    PSM_CUDA_TRY(c->st, upload(d_xl, p_xl, n_points, s));
+    PSM_CUDA_TRY(c->st, upload(d_t, p_time, n_points, s));
+    PSM_CUDA_TRY(c->st, upload(d_v, p_v, n_points, s));
+    PSM_CUDA_TRY(c->st, upload(d_lil, il_labels, c->g.n_il, s));
+    PSM_CUDA_TRY(c->st, upload(d_lxl, xl_labels, c->g.n_xl, s));
+    const size_t n = static_cast<size_t>(c->g.n_il) * c->g.n_xl * c->g.n_t;
+    psm::vrms_table_kernel<<<vrms_blocks(n), 256, 0, s>>>(
+        d_il.as<int32_t>(), d_xl.as<int32_t>(), d_t.as<double>(), d_v.as<float>(), n_points,
+        vmin, d_lil.as<int32_t>(), d_lxl.as<int32_t>(), c->g.n_il, c->g.n_xl, c->g.n_t,
+        c->g.dt_seconds, c->vrms.as<float>());
+    PSM_CUDA_TRY(c->st, cudaGetLastError());
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
+    c->have_vrms = true;
+    return PSM_OK;
+}
+
+int psm_set_vrms_grid(psm_ctx* c, const float* grid, const int32_t* g_il, int32_t g_nil,
+                      const int32_t* g_xl, int32_t g_nxl, int32_t g_nt, double g_dt,
+                      const int32_t* il_labels, const int32_t* xl_labels) {
+    if (!c || !grid || !g_il || !g_xl || g_nil <= 0 || g_nxl <= 0 || g_nt <= 0 ||
+        !(g_dt > 0.0) || !il_labels || !xl_labels)
+        return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    for (int32_t i = 1; i < g_nil; ++i)
+        if (g_il[i] <= g_il[i - 1]) return c->st.fail(PSM_ERR_ARG, "grid inlines not increasing");
+    for (int32_t i = 1; i < g_nxl; ++i)
+        if (g_xl[i] <= g_xl[i - 1])
+            return c->st.fail(PSM_ERR_ARG, "grid crosslines not increasing");
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    DevBuf d_grid, d_gil, d_gxl, d_lil, d_lxl;
+    PSM_CUDA_TRY(c->st, upload(d_grid, grid, static_cast<size_t>(g_nil) * g_nxl * g_nt, s));
+    PSM_CUDA_TRY(c->st, upload(d_gil, g_il, g_nil, s));
+    PSM_CUDA_TRY(c->st, upload(d_gxl, g_xl, g_nxl, s));
+    PSM_CUDA_TRY(c->st, upload(d_lil, il_labels, c->g.n_il, s));
+    PSM_CUDA_TRY(c->st, upload(d_lxl, xl_labels, c->g.n_xl, s));
+    const size_t n = static_cast<size_t>(c->g.n_il) * c->g.n_xl * c->g.n_t;
+    psm::vrms_grid_kernel<<<vrms_blocks(n), 256, 0, s>>>(
+        d_grid.as<float>(), d_gil.as<int32_t>(), g_nil, d_gxl.as<int32_t>(), g_nxl, g_nt, g_dt,
+        d_lil.as<int32_t>(), d_lxl.as<int32_t>(), c->g.n_il, c->g.n_xl, c->g.n_t,
+        c->g.dt_seconds, c->vrms.as<float>());
+    PSM_CUDA_TRY(c->st, cudaGetLastError());
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
+    c->have_vrms = true;
     return PSM_OK;
 }
 
@@ -755,6 +1021,680 @@ int psm_count_terms(psm_ctx* c, int64_t* n_terms) {
     *n_terms = s;
     return PSM_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------- slabs
+
+namespace {
+
+// Centre (real inline) of output inline o (main.cpp:258-288).
+inline int slab_center(const psm_geom& g, const int32_t* out_center, int o) {
+    return out_center ? out_center[o] : std::min(std::max(o - g.pad_il, 0), g.n_il - 1);
+}
+
+// Input inlines [lo, hi) output inline o reads (migration_kernel.cpp:404-409).
+inline void slab_reads(const psm_geom& g, const int32_t* out_center, int o, int* lo, int* hi) {
+    const int c = slab_center(g, out_center, o);
+    *lo = std::max(0, c - g.m_il - g.pad_il);
+    *hi = std::min(g.n_il, c + g.m_il + 1 + g.pad_il);
+}
+
+bool slab_args_ok(const psm_geom* g, const int32_t* out_center) {
+    std::string why;
+    if (!g || check_geometry(*g, &why) != PSM_OK) return false;
+    for (int o = 0; out_center && o < g->n_oi; ++o)
+        if (out_center[o] < 0 || out_center[o] >= g->n_il) return false;
+    return true;
+}
+
+// The input range of output inlines [o0, o1): the union of their reads (centres need not be
+// monotone when out_center is given).
+void slab_range(const psm_geom& g, const int32_t* out_center, psm_slab* s) {
+    s->i0 = g.n_il;
+    s->i1 = 0;
+    for (int o = s->o0; o < s->o1; ++o) {
+        int lo, hi;
+        slab_reads(g, out_center, o, &lo, &hi);
+        s->i0 = std::min(s->i0, lo);
+        s->i1 = std::max(s->i1, hi);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t psm_slab_bytes(const psm_geom* g, int32_t n_in, int32_t n_out) {
+    if (!g || n_in < 0 || n_out < 0) return -1;
+    const int64_t ns = trace_stride(g->n_t);
+    const int64_t stage = store_of(g->precision) == psm::kStoreF32 ? 8 : 4;
+    const int64_t per_trace = ns * (4 + 8) + (stage == 4 ? ns * 4 + 4 : 0) + 4LL * g->n_t;
+    return int64_t(n_in) * g->n_xl * per_trace + int64_t(n_out) * g->n_ox * g->n_t * 4 +
+           (int64_t(n_out) + n_in) * 64 + 4LL * g->n_t;
+}
+
+int psm_plan_slabs(const psm_geom* g, const int32_t* out_center, int64_t max_device_bytes,
+                   psm_slab* slabs, int32_t max_slabs, int32_t* n_slabs) {
+    if (!slab_args_ok(g, out_center) || !slabs || max_slabs <= 0 || !n_slabs) return PSM_ERR_ARG;
+    int32_t n = 0;
+    int o = 0;
+    while (o < g->n_oi) {
+        psm_slab s{o, o + 1, 0, 0};
+        slab_range(*g, out_center, &s);
+        if (max_device_bytes > 0 && psm_slab_bytes(g, s.i1 - s.i0, 1) > max_device_bytes)
+            return PSM_ERR_UNSUPPORTED;
+        while (s.o1 < g->n_oi) {  // grow while the next output inline still fits
+            psm_slab t{s.o0, s.o1 + 1, 0, 0};
+            slab_range(*g, out_center, &t);
+            if (max_device_bytes > 0 &&
+                psm_slab_bytes(g, t.i1 - t.i0, t.o1 - t.o0) > max_device_bytes)
+                break;
+            s = t;
+        }
+        if (n == max_slabs) return PSM_ERR_ARG;
+        slabs[n++] = s;
+        o = s.o1;
+    }
+    *n_slabs = n;
+    return PSM_OK;
+}
+
+int psm_split_slabs(const psm_geom* g, const int32_t* out_center, const double* weight,
+                    int32_t n_parts, psm_slab* slabs) {
+    if (!slab_args_ok(g, out_center) || n_parts <= 0 || !slabs) return PSM_ERR_ARG;
+    double total = 0.0;
+    for (int o = 0; o < g->n_oi; ++o) total += weight ? std::max(weight[o], 0.0) : 1.0;
+    int o = 0;
+    double acc = 0.0;
+    for (int32_t k = 0; k < n_parts; ++k) {
+        psm_slab s{o, o, 0, 0};
+        const double target = total * (k + 1) / n_parts;
+        // take output inlines while the running work stays closest to the k-th quantile
+        while (s.o1 < g->n_oi) {
+            const double w = weight ? std::max(weight[s.o1], 0.0) : 1.0;
+            if (k == n_parts - 1 || acc + w <= target || acc + 0.5 * w <= target) {
+                acc += w;
+                ++s.o1;
+            } else {
+                break;
+            }
+        }
+        slab_range(*g, out_center, &s);
+        if (s.o1 == s.o0) s.i0 = s.i1 = 0;
+        slabs[k] = s;
+        o = s.o1;
+    }
+    return PSM_OK;
+}
+
+int psm_slab_geometry(const psm_geom* g, const int32_t* out_center, const psm_slab* s,
+                      psm_geom* local, int32_t* local_center) {
+    if (!slab_args_ok(g, out_center) || !s || !local || !local_center) return PSM_ERR_ARG;
+    if (s->o0 < 0 || s->o1 > g->n_oi || s->o0 >= s->o1) return PSM_ERR_ARG;
+    psm_slab need{s->o0, s->o1, 0, 0};
+    slab_range(*g, out_center, &need);
+    if (s->i0 < 0 || s->i1 > g->n_il || s->i0 > need.i0 || s->i1 < need.i1) return PSM_ERR_ARG;
+    *local = *g;
+    local->n_il = s->i1 - s->i0;
+    local->n_oi = s->o1 - s->o0;
+    for (int o = s->o0; o < s->o1; ++o)
+        local_center[o - s->o0] = slab_center(*g, out_center, o) - s->i0;
+    return PSM_OK;
+}
+
+int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_center,
+                         const float* traces, const float* vrms, float* image,
+                         int64_t max_device_bytes) {
+    if (!c || !traces || !vrms || !image) return PSM_ERR_ARG;
+    if (!slab_args_ok(g, out_center)) return c->st.fail(PSM_ERR_ARG, "invalid geometry");
+    std::vector<psm_slab> slabs(static_cast<size_t>(g->n_oi));
+    int32_t n = 0;
+    int rc = psm_plan_slabs(g, out_center, max_device_bytes, slabs.data(), g->n_oi, &n);
+    if (rc) return c->st.fail(rc, "one output inline exceeds the device budget");
+    const size_t trace = static_cast<size_t>(g->n_xl) * g->n_t;
+    const size_t row = static_cast<size_t>(g->n_ox) * g->n_t;
+    for (int32_t k = 0; k < n; ++k) {
+        const psm_slab& s = slabs[k];
+        psm_geom local;
+        std::vector<int32_t> lc(static_cast<size_t>(s.o1 - s.o0));
+        if ((rc = psm_slab_geometry(g, out_center, &s, &local, lc.data()))) return rc;
+        if ((rc = psm_set_geometry(c, &local, lc.data()))) return rc;
+        if ((rc = psm_set_traces(c, traces + s.i0 * trace))) return rc;
+        if ((rc = psm_set_vrms(c, vrms + s.i0 * trace))) return rc;
+        if ((rc = psm_forward(c, image + s.o0 * row))) return rc;
+    }
+    return PSM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------- batched launch
+
+namespace {
+
+struct BatchCube {
+    const float* host = nullptr;
+    int n_il = 0, n_xl = 0, n_t = 0, ns = 0;
+    DevBuf data, pairs, words, scales;
+};
+
+struct BatchProblem {
+    psm_problem src{};
+    int cube = 0;
+    std::vector<Job> jobs, jobs_all;
+    std::vector<std::pair<int, int>> copies;
+    DevBuf vrms, image, d_jobs, d_jobs_all, t0;
+    FwdParams P{};
+};
+
+}  // namespace
+
+struct psm_batch {
+    psm_ctx* ctx = nullptr;
+    std::vector<BatchCube> cubes;
+    std::vector<BatchProblem> probs;
+    int store = psm::kStoreF32;
+    bool amp = true, kahan = false;
+    int variant = PSM_FWD_DEFAULT;
+    int mode = PSM_BATCH_PERSISTENT;
+    int max_inl = 1, stage_cap = 0;
+    int grid = 1;  // persistent CTAs
+    int order = PSM_ORDER_DEPTH_FIRST;
+    // tile lists [time tile 256 / 512 samples (8 / 16 blocks a lane)][order]
+    int n_items[4] = {0, 0, 0, 0};
+    DevBuf items[4];
+    std::unique_ptr<psm::BatchParams> params;  // every problem's FwdParams (kernel argument)
+    DevBuf counter, il_pos;
+    cudaGraphExec_t exec = nullptr;
+    int exec_key = -1;  // variant and order the graph was captured with
+    int64_t n_terms = -1;
+    ~psm_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
+namespace {
+
+// Shared-memory attribute and persistent grid (resident CTAs on every SM) of the batch
+// kernel K; done before a stream capture, so the graph holds only the launch.
+template <class K>
+cudaError_t prepare_persistent(K, psm_batch& b) {
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+    const size_t smem =
+        psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, n_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * (psm::kTX + 1), smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, b.ctx->device);
+    if (e != cudaSuccess) return e;
+    const int w = (K::J == 16 ? 2 : 0) + b.order;
+    b.grid = std::max(1, std::min(b.n_items[w], n_sm * std::max(per_sm, 1)));
+    return cudaSuccess;
+}
+
+template <class K>
+cudaError_t launch_persistent(K, const psm_batch& b, cudaStream_t s) {
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+    const size_t smem =
+        psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
+    const int w = (K::J == 16 ? 2 : 0) + b.order;
+    kern<<<b.grid, 32 * (psm::kTX + 1), smem, s>>>(
+        *b.params, b.items[w].as<psm::BatchItem>(), b.n_items[w], b.counter.as<int>(),
+        b.ctx->err.as<int>(), b.max_inl, b.stage_cap);
+    return cudaGetLastError();
+}
+
+// Repeated output rows of every problem (padded output inlines, main.cpp:268-285).
+cudaError_t batch_copies(const psm_batch& b, cudaStream_t s) {
+    for (const BatchProblem& p : b.probs) {
+        const size_t row = static_cast<size_t>(p.src.geom.n_ox) * p.src.geom.n_t;
+        for (const auto& cp : p.copies) {
+            cudaError_t e = cudaMemcpyAsync(p.image.as<float>() + cp.first * row,
+                                            p.image.as<float>() + cp.second * row,
+                                            row * sizeof(float), cudaMemcpyDeviceToDevice, s);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+// The work of one batched run, enqueued on s (persistent: counter and error word reset, one
+// launch, row copies).
+cudaError_t batch_enqueue(psm_batch& b, int variant, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(b.ctx->err.p, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    if (b.mode == PSM_BATCH_PER_PROBLEM) {
+        for (const BatchProblem& p : b.probs) {
+            e = launch_fwd(p.P, static_cast<int>(p.jobs.size()), b.amp, variant, s, b.store,
+                           b.kahan);
+            if (e != cudaSuccess) return e;
+        }
+    } else {
+        e = cudaMemsetAsync(b.counter.p, 0, sizeof(int), s);
+        if (e != cudaSuccess) return e;
+        e = with_kernel(b.amp, variant, b.store, b.kahan,
+                        [&](auto k) { return launch_persistent(k, b, s); });
+        if (e != cudaSuccess) return e;
+    }
+    return batch_copies(b, s);
+}
+
+// Capture the run (either mode) into a CUDA graph once per variant, order and mode, then
+// replay it.
+int batch_launch(psm_batch* b) {
+    psm_ctx* c = b->ctx;
+    const int v = effective_variant(b->variant, b->store, b->kahan);
+    const int key = (v * 2 + b->order) * 2 + b->mode;
+    if (!b->exec || b->exec_key != key) {
+        if (b->exec) {
+            cudaGraphExecDestroy(b->exec);
+            b->exec = nullptr;
+        }
+        if (b->mode == PSM_BATCH_PERSISTENT)
+            PSM_CUDA_TRY(c->st, with_kernel(b->amp, v, b->store, b->kahan, [&](auto k) {
+                             return prepare_persistent(k, *b);
+                         }));
+        else {  // grid launches: the shared-memory attribute is set outside the capture
+            size_t smem = 0;
+            for (const BatchProblem& p : b->probs) smem = std::max(smem, fwd_smem(p.P, b->store));
+            PSM_CUDA_TRY(c->st, with_kernel(b->amp, v, b->store, b->kahan,
+                                            [&](auto k) { return prepare_grid(k, smem); }));
+        }
+        cudaGraph_t graph = nullptr;
+        PSM_CUDA_TRY(c->st, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e = batch_enqueue(*b, v, c->stream);
+        const cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+        PSM_CUDA_TRY(c->st, e);
+        PSM_CUDA_TRY(c->st, e2);
+        const cudaError_t e3 = cudaGraphInstantiate(&b->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        PSM_CUDA_TRY(c->st, e3);
+        b->exec_key = key;
+    }
+    PSM_CUDA_TRY(c->st, cudaGraphLaunch(b->exec, c->stream));
+    return PSM_OK;
+}
+
+// Upload (or re-upload) every cube and Vrms from the host arrays.
+int batch_upload(psm_batch* b) {
+    psm_ctx* c = b->ctx;
+    cudaStream_t s = c->stream;
+    for (BatchCube& q : b->cubes) {
+        const size_t n_tr = static_cast<size_t>(q.n_il) * q.n_xl;
+        PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(q.data.p, q.ns * sizeof(float), q.host,
+                                              q.n_t * sizeof(float), q.n_t * sizeof(float),
+                                              n_tr, cudaMemcpyHostToDevice, s));
+        if (b->store == psm::kStoreF32)
+            PSM_CUDA_TRY(c->st, build_pairs(q.data.as<float>(), q.pairs.as<float2>(), n_tr,
+                                            q.ns, s));
+        else
+            PSM_CUDA_TRY(c->st, quantize(q.data.as<float>(), q.words.as<uint32_t>(),
+                                         q.scales.as<float>(), n_tr, q.ns, b->store, s));
+    }
+    for (BatchProblem& p : b->probs) {
+        const psm_geom& g = p.src.geom;
+        if (p.src.vrms_kind == PSM_VRMS_CUBE) {
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.vrms.p, p.src.vrms,
+                                                static_cast<size_t>(g.n_il) * g.n_xl * g.n_t *
+                                                    sizeof(float),
+                                                cudaMemcpyHostToDevice, s));
+        } else if (p.src.vrms_kind == PSM_VRMS_TRACE) {
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.vrms.p, p.src.vrms, g.n_t * sizeof(float),
+                                                cudaMemcpyHostToDevice, s));
+        }
+    }
+    return PSM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psm_batch_create(psm_ctx* c, const psm_problem* problems, int n, psm_batch** out) {
+    if (!c || !problems || n <= 0 || !out) return PSM_ERR_ARG;
+    *out = nullptr;
+    if (n > psm::kMaxBatchProblems)
+        return c->st.fail(PSM_ERR_UNSUPPORTED, "at most " +
+                                                   std::to_string(psm::kMaxBatchProblems) +
+                                                   " problems per batch");
+    cudaSetDevice(c->device);
+    std::unique_ptr<psm_batch> b(new (std::nothrow) psm_batch());
+    if (!b) return PSM_ERR_NOMEM;
+    b->ctx = c;
+    b->probs.resize(n);
+    const psm_geom& g0 = problems[0].geom;
+    b->store = store_of(g0.precision);
+    b->amp = g0.amp_correction != 0;
+    b->kahan = g0.compensated != 0;
+    int max_il = 1;
+    for (int i = 0; i < n; ++i) {
+        const psm_problem& src = problems[i];
+        const psm_geom& g = src.geom;
+        std::string why;
+        int rc = check_geometry(g, &why);
+        if (rc) return c->st.fail(rc, "problem " + std::to_string(i) + ": " + why);
+        if ((g.amp_correction != 0) != b->amp || g.precision != g0.precision ||
+            (g.compensated != 0) != b->kahan)
+            return c->st.fail(PSM_ERR_ARG, "problems differ in amp_correction, precision or "
+                                           "compensated");
+        if (!src.traces || (src.vrms_kind != PSM_VRMS_CONSTANT && !src.vrms) ||
+            src.vrms_kind < PSM_VRMS_CUBE || src.vrms_kind > PSM_VRMS_CONSTANT ||
+            (src.vrms_kind == PSM_VRMS_CONSTANT && !(src.velocity >= 0.0f)))
+            return c->st.fail(PSM_ERR_ARG, "problem " + std::to_string(i) +
+                                               ": traces / vrms / velocity");
+        BatchProblem& p = b->probs[i];
+        p.src = src;
+        if (!plan_jobs(g, src.out_center, p.jobs, p.jobs_all, p.copies))
+            return c->st.fail(PSM_ERR_ARG, "problem " + std::to_string(i) +
+                                               ": out_center out of range");
+        // cube shared with an earlier problem given the same host array and grid
+        int cube = -1;
+        for (size_t k = 0; k < b->cubes.size(); ++k) {
+            const BatchCube& q = b->cubes[k];
+            if (q.host == src.traces && q.n_il == g.n_il && q.n_xl == g.n_xl && q.n_t == g.n_t)
+                cube = static_cast<int>(k);
+        }
+        if (cube < 0) {
+            cube = static_cast<int>(b->cubes.size());
+            b->cubes.emplace_back();
+            BatchCube& q = b->cubes.back();
+            q.host = src.traces;
+            q.n_il = g.n_il;
+            q.n_xl = g.n_xl;
+            q.n_t = g.n_t;
+            q.ns = trace_stride(g.n_t);
+        }
+        p.cube = cube;
+        max_il = std::max(max_il, g.n_il);
+        b->max_inl = std::max(b->max_inl, max_inline_window(p.jobs_all));
+        b->stage_cap = std::max(b->stage_cap, stage_cap(trace_stride(g.n_t), b->store));
+    }
+    if (psm::smem_layout(b->max_inl, b->stage_cap, psm::store_bytes(b->store)).total >
+        kMaxDynSmem)
+        return c->st.fail(PSM_ERR_UNSUPPORTED, "problems too large for one staging ring");
+    cudaStream_t s = c->stream;
+    PSM_CUDA_TRY(c->st, c->err.ensure(sizeof(int)));
+    for (BatchCube& q : b->cubes) {
+        const size_t n = static_cast<size_t>(q.n_il) * q.n_xl * q.ns;
+        PSM_CUDA_TRY(c->st, q.data.ensure(n * sizeof(float)));
+        PSM_CUDA_TRY(c->st, cudaMemsetAsync(q.data.p, 0, n * sizeof(float), s));
+        if (b->store == psm::kStoreF32) {
+            PSM_CUDA_TRY(c->st, q.pairs.ensure(n * sizeof(float2)));
+        } else {
+            PSM_CUDA_TRY(c->st, q.words.ensure(n * sizeof(uint32_t)));
+            PSM_CUDA_TRY(c->st, q.scales.ensure(static_cast<size_t>(q.n_il) * q.n_xl *
+                                                sizeof(float)));
+        }
+    }
+    std::vector<int> pos(max_il);
+    for (int i = 0; i < max_il; ++i) pos[i] = i;
+    PSM_CUDA_TRY(c->st, b->il_pos.ensure(max_il * sizeof(int)));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(b->il_pos.p, pos.data(), max_il * sizeof(int),
+                                        cudaMemcpyHostToDevice, s));
+    b->params.reset(new (std::nothrow) psm::BatchParams());
+    if (!b->params) return PSM_ERR_NOMEM;
+    std::vector<std::vector<float>> host_t0(n), host_v(n);
+    for (int i = 0; i < n; ++i) {
+        BatchProblem& p = b->probs[i];
+        const psm_geom& g = p.src.geom;
+        const BatchCube& q = b->cubes[p.cube];
+        const int vk = p.src.vrms_kind;
+        const size_t nv = vk == PSM_VRMS_CUBE ? static_cast<size_t>(g.n_il) * g.n_xl * g.n_t
+                                              : static_cast<size_t>(g.n_t);
+        PSM_CUDA_TRY(c->st, p.vrms.ensure(nv * sizeof(float)));
+        PSM_CUDA_TRY(c->st, p.image.ensure(static_cast<size_t>(g.n_oi) * g.n_ox * g.n_t *
+                                           sizeof(float)));
+        PSM_CUDA_TRY(c->st, p.d_jobs.ensure(p.jobs.size() * sizeof(Job)));
+        PSM_CUDA_TRY(c->st, p.d_jobs_all.ensure(p.jobs_all.size() * sizeof(Job)));
+        PSM_CUDA_TRY(c->st, p.t0.ensure(g.n_t * sizeof(float)));
+        host_t0[i].resize(g.n_t);
+        for (int t = 0; t < g.n_t; ++t)
+            host_t0[i][t] = static_cast<float>(static_cast<double>(t) * g.dt_seconds);
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.t0.p, host_t0[i].data(), g.n_t * sizeof(float),
+                                            cudaMemcpyHostToDevice, s));
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.d_jobs.p, p.jobs.data(), p.jobs.size() * sizeof(Job),
+                                            cudaMemcpyHostToDevice, s));
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.d_jobs_all.p, p.jobs_all.data(),
+                                            p.jobs_all.size() * sizeof(Job),
+                                            cudaMemcpyHostToDevice, s));
+        if (vk == PSM_VRMS_CONSTANT) {
+            host_v[i].assign(g.n_t, p.src.velocity);
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.vrms.p, host_v[i].data(), g.n_t * sizeof(float),
+                                                cudaMemcpyHostToDevice, s));
+        }
+        FwdParams& P = p.P;
+        P.pairs = q.pairs.as<float2>();
+        P.words = q.words.as<uint32_t>();
+        P.scales = q.scales.as<float>();
+        P.vrms = p.vrms.as<float>();
+        P.image = p.image.as<float>();
+        P.jobs = p.d_jobs.as<Job>();
+        P.il_pos = b->il_pos.as<int>();
+        P.t0 = p.t0.as<float>();
+        P.err = c->err.as<int>();
+        P.n_ci = g.n_il;
+        P.n_cx = g.n_xl;
+        P.n_t = g.n_t;
+        P.ns = q.ns;
+        P.n_vx = g.n_xl;
+        P.n_ox = g.n_ox;
+        P.xoff = -g.pad_xl;
+        P.max_inl = max_inline_window(p.jobs_all);
+        P.stage_cap = stage_cap(q.ns, b->store);
+        fill_consts(P, g.dt, g.d_il, g.d_xl, g.tan2_theta);
+        if (vk != PSM_VRMS_CUBE) P.vs_x = P.vs_row = 0;  // one Vrms trace for every point
+        b->params->p[i] = P;
+    }
+    // tile lists, for 256- and 512-sample time tiles, in two orders:
+    //  * depth first: deepest time tiles first (the aperture, and so the work, grows with
+    //    t0), then output inline, crossline tile and problem, so panels over one cube take
+    //    the same tile one after another and the long tiles start early;
+    //  * problem after problem, each in the grid kernel's order (crossline tile fastest,
+    //    then time tile, then output inline).
+    PSM_CUDA_TRY(c->st, b->counter.ensure(sizeof(int)));
+    for (int w = 0; w < 4; ++w) {
+        const int TT = 32 * (w >= 2 ? 16 : 8);
+        std::vector<psm::BatchItem> items;
+        for (int i = 0; i < n; ++i) {
+            const BatchProblem& p = b->probs[i];
+            const psm_geom& g = p.src.geom;
+            for (int j = 0; j < static_cast<int>(p.jobs.size()); ++j)
+                for (int T0 = 0; T0 < g.n_t; T0 += TT)
+                    for (int x0 = 0; x0 < g.n_ox; x0 += psm::kTX) items.push_back({i, j, x0, T0});
+        }
+        if ((w & 1) == PSM_ORDER_DEPTH_FIRST)
+            std::stable_sort(items.begin(), items.end(),
+                             [](const psm::BatchItem& a, const psm::BatchItem& z) {
+                                 if (a.T0 != z.T0) return a.T0 > z.T0;
+                                 if (a.job != z.job) return a.job < z.job;
+                                 if (a.x0 != z.x0) return a.x0 < z.x0;
+                                 return a.prob < z.prob;
+                             });
+        b->n_items[w] = static_cast<int>(items.size());
+        PSM_CUDA_TRY(c->st, b->items[w].ensure(items.size() * sizeof(psm::BatchItem)));
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(b->items[w].p, items.data(),
+                                            items.size() * sizeof(psm::BatchItem),
+                                            cudaMemcpyHostToDevice, s));
+        PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));  // items is released next iteration
+    }
+    int rc = batch_upload(b.get());
+    if (rc) return rc;
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
+    *out = b.release();
+    return PSM_OK;
+}
+
+int psm_batch_destroy(psm_batch* b) {
+    if (!b) return PSM_OK;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    delete b;
+    return PSM_OK;
+}
+
+int psm_batch_reload(psm_batch* b) {
+    if (!b) return PSM_ERR_ARG;
+    cudaSetDevice(b->ctx->device);
+    return batch_upload(b);
+}
+
+int psm_batch_get_mode(psm_batch* b, int* mode) {
+    if (!b || !mode) return PSM_ERR_ARG;
+    *mode = b->mode;
+    return PSM_OK;
+}
+
+int psm_batch_set_mode(psm_batch* b, int mode) {
+    if (!b || (mode != PSM_BATCH_PERSISTENT && mode != PSM_BATCH_PER_PROBLEM))
+        return PSM_ERR_ARG;
+    b->mode = mode;
+    return PSM_OK;
+}
+
+int psm_batch_set_order(psm_batch* b, int order) {
+    if (!b || (order != PSM_ORDER_DEPTH_FIRST && order != PSM_ORDER_PROBLEM)) return PSM_ERR_ARG;
+    b->order = order;
+    return PSM_OK;
+}
+
+int psm_batch_get_order(psm_batch* b, int* order) {
+    if (!b || !order) return PSM_ERR_ARG;
+    *order = b->order;
+    return PSM_OK;
+}
+
+int psm_batch_set_variant(psm_batch* b, int variant) {
+    if (!b || variant < 0 || variant >= PSM_FWD_N_VARIANTS) return PSM_ERR_ARG;
+    b->variant = variant;
+    return PSM_OK;
+}
+
+int psm_batch_get_variant(psm_batch* b, int* variant) {
+    if (!b || !variant) return PSM_ERR_ARG;
+    *variant = effective_variant(b->variant, b->store, b->kahan);
+    return PSM_OK;
+}
+
+int psm_batch_run_async(psm_batch* b) {
+    if (!b) return PSM_ERR_ARG;
+    cudaSetDevice(b->ctx->device);
+    return batch_launch(b);
+}
+
+int psm_batch_synchronize(psm_batch* b) {
+    if (!b) return PSM_ERR_ARG;
+    return psm_synchronize(b->ctx);
+}
+
+int psm_batch_run(psm_batch* b) {
+    int r = psm_batch_run_async(b);
+    return r ? r : psm_batch_synchronize(b);
+}
+
+int psm_batch_autotune(psm_batch* b, float* ms, int* best, int* best_order, int* best_mode) {
+    if (!b) return PSM_ERR_ARG;
+    psm_ctx* c = b->ctx;
+    cudaSetDevice(c->device);
+    if (ms)
+        for (int v = 0; v < 3 * PSM_FWD_N_VARIANTS; ++v) ms[v] = 0.0f;
+    cudaEvent_t e0, e1;
+    PSM_CUDA_TRY(c->st, cudaEventCreate(&e0));
+    PSM_CUDA_TRY(c->st, cudaEventCreate(&e1));
+    int pick = effective_variant(PSM_FWD_DEFAULT, b->store, b->kahan);
+    int pick_order = b->order, pick_mode = b->mode;
+    float pick_ms = 3.0e38f;
+    int rc = PSM_OK;
+    // schedules: persistent depth-first, persistent problem order, one launch per problem
+    for (int sch = 0; sch < 3 && rc == PSM_OK; ++sch) {
+        b->mode = sch < 2 ? PSM_BATCH_PERSISTENT : PSM_BATCH_PER_PROBLEM;
+        b->order = sch < 2 ? sch : PSM_ORDER_DEPTH_FIRST;
+        for (int v = 1; v < PSM_FWD_N_VARIANTS && rc == PSM_OK; ++v) {
+            if (effective_variant(v, b->store, b->kahan) != v) continue;  // same kernel
+            b->variant = v;
+            float t = 0.0f;
+            if ((rc = psm_batch_run(b)) != PSM_OK) break;  // warm: graph capture, first launch
+            cudaEventRecord(e0, c->stream);
+            if ((rc = batch_launch(b)) != PSM_OK) break;
+            cudaEventRecord(e1, c->stream);
+            if ((rc = psm_batch_synchronize(b)) != PSM_OK) break;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (ms) ms[sch * PSM_FWD_N_VARIANTS + v] = t;
+            if (t < pick_ms) {
+                pick_ms = t;
+                pick = v;
+                pick_order = b->order;
+                pick_mode = b->mode;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->variant = pick;
+    b->order = pick_order;
+    b->mode = pick_mode;
+    if (rc == PSM_OK && best) *best = pick;
+    if (rc == PSM_OK && best_order) *best_order = pick_order;
+    if (rc == PSM_OK && best_mode) *best_mode = pick_mode;
+    return rc;
+}
+
+int psm_batch_image_device(psm_batch* b, int i, float** dev) {
+    if (!b || !dev || i < 0 || i >= static_cast<int>(b->probs.size())) return PSM_ERR_ARG;
+    *dev = b->probs[i].image.as<float>();
+    return PSM_OK;
+}
+
+int psm_batch_get_image(psm_batch* b, int i, float* image) {
+    if (!b || !image || i < 0 || i >= static_cast<int>(b->probs.size())) return PSM_ERR_ARG;
+    psm_ctx* c = b->ctx;
+    cudaSetDevice(c->device);
+    const psm_geom& g = b->probs[i].src.geom;
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image, b->probs[i].image.p,
+                                        static_cast<size_t>(g.n_oi) * g.n_ox * g.n_t *
+                                            sizeof(float),
+                                        cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int psm_batch_count_terms(psm_batch* b, int64_t* n_terms) {
+    if (!b || !n_terms) return PSM_ERR_ARG;
+    psm_ctx* c = b->ctx;
+    cudaSetDevice(c->device);
+    if (b->n_terms < 0) {
+        size_t nj = 0;
+        for (const BatchProblem& p : b->probs) nj += p.jobs_all.size();
+        PSM_CUDA_TRY(c->st, c->count.ensure(nj * sizeof(unsigned long long)));
+        PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->count.p, 0, nj * sizeof(unsigned long long),
+                                            c->stream));
+        size_t off = 0;
+        for (const BatchProblem& p : b->probs) {
+            FwdParams P = p.P;
+            P.jobs = p.d_jobs_all.as<Job>();
+            psm::count_kernel<<<dim3(p.src.geom.n_ox, static_cast<unsigned>(p.jobs_all.size())),
+                                256, 0, c->stream>>>(P, c->count.as<unsigned long long>() + off);
+            PSM_CUDA_TRY(c->st, cudaGetLastError());
+            off += p.jobs_all.size();
+        }
+        std::vector<unsigned long long> h(nj);
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(h.data(), c->count.p, nj * sizeof(unsigned long long),
+                                            cudaMemcpyDeviceToHost, c->stream));
+        PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
+        int64_t s = 0;
+        for (unsigned long long v : h) s += static_cast<int64_t>(v);
+        b->n_terms = s;
+    }
+    *n_terms = b->n_terms;
+    return PSM_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
 
 // ---------------------------------------------------------------------------- per inline
 

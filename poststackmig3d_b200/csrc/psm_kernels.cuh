@@ -539,7 +539,7 @@ __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2
 // of a persistent CTA continue the ring's phases (every stage, the end-of-stream marker
 // included, is released by the consumers).  Returns false when a bounded wait expired.
 template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN>
-__device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job& job, int x0, int T0,
+__device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int x0, int T0,
                                          unsigned char* smem_raw, const SmemLayout& L,
                                          uint32_t& it) {
     static_assert(GB == 2 || GB == 4, "skip groups of 2 or 4 blocks");
@@ -547,7 +547,6 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job& job, int
     static_assert(STORE == kStoreF32 || PACKED, "16-bit storage uses packed arithmetic");
     constexpr int NG = J / GB;   // skip groups per lane
     constexpr int PG = GB / 2;   // block pairs per group
-    constexpr int TT = 32 * J;   // output samples per tile
     constexpr int EB = store_bytes(STORE);
     // bits(2^23) << log2(EB), modulo 2^32 (see the producer)
     constexpr uint32_t MAGIC = EB == 8 ? 0x58000000u : 0x2C000000u;
@@ -566,6 +565,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job& job, int
     float2(&SUM)[J / 2] = KAHAN ? PART : ACC;
     float gmax[NG], gmin[NG];
     float warpmax = -1.0f;
+    float gminall = 3.0e38f;  // every lane of every group passes when r2 <= gminall
     const int x = x0 + warp - 1;
     const int xv = x + P.xoff;
     if (warp > 0) {
@@ -620,6 +620,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job& job, int
             gmax[g] = warp_max(mx);
             gmin[g] = warp_min(mn);
             warpmax = fmaxf(warpmax, gmax[g]);
+            gminall = fminf(gminall, gmin[g]);
         }
         vmin = warp_min(vmin);
         vmax = warp_max(vmax);
@@ -819,14 +820,28 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job& job, int
             const uint32_t base2 = static_cast<uint32_t>(md.z);
             Win w;
             w.wsf = __int_as_float(md.w);
-            w.shi = m.shi[g];
 #ifdef PSM_DEBUG_BOUNDS
+            w.shi = m.shi[g];
             w.wef = m.wend[g];
 #else
+            w.shi = 0.0f;  // read below, where a clamp needs it
             w.wef = 0.0f;
 #endif
             w.err = P.err;
             const float sc = STORE == kStoreF32 ? 1.0f : m.sc[g];
+            if (r2 <= gminall) {  // interior trace: every term of the tile passes
+#pragma unroll
+                for (int p = 0; p < J / 2; ++p) {
+                    if (STORE == kStoreF32)
+                        term_pair<AMP, false, PACKED>(smem_raw, r2, base2, w, T2[p], F4[p],
+                                                      BB[p], SUM[p]);
+                    else
+                        term_pair16<AMP, false, STORE>(smem_raw, r2, base2, w, sc, T2[p],
+                                                       F4[p], BB[p], SUM[p]);
+                }
+                continue;
+            }
+            w.shi = m.shi[g];
 #pragma unroll
             for (int gr = 0; gr < NG; ++gr) {
                 if (r2 <= gmax[gr]) {
@@ -922,19 +937,26 @@ struct BatchItem {
     int prob, job, x0, T0;
 };
 
+// Parameters of every problem of a batched launch, passed by value: they live in the
+// kernel-parameter constant bank, whose loads are cached and uniform across the CTA.
+constexpr int kMaxBatchProblems = 192;
+struct BatchParams {
+    FwdParams p[kMaxBatchProblems];
+};
+static_assert(sizeof(BatchParams) + 64 <= 32764, "kernel parameters are limited to 32764 bytes");
+
 // Persistent batched launch: each CTA takes tiles from the shared list in order (an atomic
 // counter) until the list is exhausted, with the ring kept across tiles.  Problems (velocity
-// panels, sub-volumes) each have their own FwdParams; the CTA copies the current problem's
-// parameters to shared memory.  max_inl and stage_cap are the largest over the problems.
-// A device error (bounded wait expired) stops every CTA at its next tile.
+// panels, sub-volumes) each have their own FwdParams.  max_inl and stage_cap are the largest
+// over the problems.  A device error (bounded wait expired) stops every CTA at its next tile.
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2)
-    fwd_batch_kernel(const FwdParams* __restrict__ probs, const BatchItem* __restrict__ items,
-                     int n_items, int* next, const int* err, int max_inl, int stage_cap) {
+    fwd_batch_kernel(const __grid_constant__ BatchParams B,
+                     const BatchItem* __restrict__ items, int n_items, int* next,
+                     const int* err, int max_inl, int stage_cap) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ FwdParams s_P;
-    __shared__ Job s_job;
     __shared__ BatchItem s_item;
+    __shared__ Job s_job;
     const SmemLayout L = smem_layout(max_inl, stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
@@ -943,16 +965,14 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2)
             const int k = *reinterpret_cast<const volatile int*>(err) ? n_items
                                                                       : atomicAdd(next, 1);
             s_item = k < n_items ? items[k] : BatchItem{-1, 0, 0, 0};
-            if (k < n_items) {
-                s_P = probs[s_item.prob];
-                s_job = s_P.jobs[s_item.job];
-            }
+            if (k < n_items) s_job = B.p[s_item.prob].jobs[s_item.job];
         }
         __syncthreads();
-        if (s_item.prob < 0) break;
-        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(s_P, s_job, s_item.x0,
-                                                                  s_item.T0, smem_raw, L, it);
-        // barrier: the tile's tables, statistics and s_P are reused next
+        const BatchItem w = s_item;
+        if (w.prob < 0) break;
+        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(B.p[w.prob], s_job, w.x0,
+                                                                  w.T0, smem_raw, L, it);
+        // barrier: the tile's tables, statistics, s_item and s_job are reused next
         if (__syncthreads_or(!ok)) break;
     }
 }

@@ -202,6 +202,76 @@ class Migrator:
             data = _f32(data, (g.n_il, g.n_xl, g.n_t))
         check(self._L.psm_set_traces(self._ctx, _addr(data)), self._err)
 
+    def set_vrms_table(self, points, il_labels, xl_labels) -> None:
+        """Vrms from a text table's points [(il, xl, time_s, v), ...], assembled on the GPU."""
+        pts = list(points)
+        p_il = np.array([p[0] for p in pts], dtype=np.int32)
+        p_xl = np.array([p[1] for p in pts], dtype=np.int32)
+        p_t = np.array([p[2] for p in pts], dtype=np.float64)
+        p_v = np.array([p[3] for p in pts], dtype=np.float32)
+        il = np.ascontiguousarray(il_labels, dtype=np.int32)
+        xl = np.ascontiguousarray(xl_labels, dtype=np.int32)
+        check(self._L.psm_set_vrms_table(self._ctx, p_il.ctypes.data, p_xl.ctypes.data,
+                                         p_t.ctypes.data, p_v.ctypes.data, len(pts),
+                                         il.ctypes.data, xl.ctypes.data), self._err)
+
+    def set_vrms_grid(self, grid, g_il, g_xl, g_dt: float, il_labels, xl_labels) -> None:
+        """Vrms from a SEG-Y Vrms grid [g_nil][g_nxl][g_nt] (sorted labels), on the GPU."""
+        gr = _f32(grid)
+        gi = np.ascontiguousarray(g_il, dtype=np.int32)
+        gx = np.ascontiguousarray(g_xl, dtype=np.int32)
+        il = np.ascontiguousarray(il_labels, dtype=np.int32)
+        xl = np.ascontiguousarray(xl_labels, dtype=np.int32)
+        check(self._L.psm_set_vrms_grid(self._ctx, gr.ctypes.data, gi.ctypes.data, len(gi),
+                                        gx.ctypes.data, len(gx), gr.shape[2], float(g_dt),
+                                        il.ctypes.data, xl.ctypes.data), self._err)
+
+    def get_vrms(self) -> np.ndarray:
+        g = self.geom
+        out = np.empty((g.n_il, g.n_xl, g.n_t), dtype=np.float32)
+        check(self._L.psm_get_vrms(self._ctx, out.ctypes.data), self._err)
+        return out
+
+    def set_traces_segy(self, records, format: int, position) -> None:
+        """Upload SEG-Y trace records (uint8 [n_records][240 + 4 n_t], as in the file after
+        its 3600 header bytes) and decode them on the GPU into the resident cube; record r
+        fills cube trace position[r] (il_index * n_xl + xl_index) or nothing (-1)."""
+        rec = np.ascontiguousarray(records, dtype=np.uint8)
+        n_t = self.geom.n_t
+        n = rec.size // (240 + 4 * n_t)
+        if rec.size != n * (240 + 4 * n_t):
+            raise ValueError("records are not whole traces of 240 + 4 n_t bytes")
+        pos = np.ascontiguousarray(position, dtype=np.int32)
+        if pos.size != n:
+            raise ValueError("one position per record")
+        check(self._L.psm_set_traces_segy(self._ctx, rec.ctypes.data, n, int(format),
+                                          pos.ctypes.data), self._err)
+
+    def get_image_segy(self, format: int, source, il_label, xl_label) -> np.ndarray:
+        """The image as output SEG-Y trace records (uint8 [n_oi * n_ox][240 + 4 n_t])."""
+        g = self.geom
+        out = np.empty((g.n_oi * g.n_ox, 240 + 4 * g.n_t), dtype=np.uint8)
+        src = np.ascontiguousarray(source, dtype=np.int32)
+        il = np.ascontiguousarray(il_label, dtype=np.int32)
+        xl = np.ascontiguousarray(xl_label, dtype=np.int32)
+        if src.size != g.n_oi * g.n_ox or il.size != g.n_oi or xl.size != g.n_ox:
+            raise ValueError("source [n_oi * n_ox], il_label [n_oi], xl_label [n_ox]")
+        check(self._L.psm_get_image_segy(self._ctx, out.ctypes.data, int(format),
+                                         src.ctypes.data, il.ctypes.data, xl.ctypes.data),
+              self._err)
+        return out
+
+    def get_traces(self) -> np.ndarray:
+        g = self.geom
+        out = np.empty((g.n_il, g.n_xl, g.n_t), dtype=np.float32)
+        check(self._L.psm_get_traces(self._ctx, out.ctypes.data), self._err)
+        return out
+
+    def set_image(self, image) -> None:
+        g = self.geom
+        img = _f32(image, (g.n_oi, g.n_ox, g.n_t))
+        check(self._L.psm_set_image(self._ctx, img.ctypes.data), self._err)
+
     def set_vrms(self, vrms) -> None:
         g = self.geom
         if isinstance(vrms, np.ndarray):
@@ -293,6 +363,149 @@ class Migrator:
         out = np.zeros(self.geom.n_oi, dtype=np.int64)
         check(self._L.psm_count_terms_rows(self._ctx, out.ctypes.data), self._err)
         return out
+
+
+class Problem:
+    """One problem of a batched launch: a cube, its Vrms and its geometry.
+
+    vrms: a [n_il][n_xl][n_t] cube, a [n_t] trace used for every output point, or None with
+    velocity set (a constant-velocity scan panel).  Problems given the same traces array
+    share one device copy of it."""
+
+    def __init__(self, geom: Geometry, traces, vrms=None, velocity: float = 0.0):
+        self.geom = geom
+        self.traces = _f32(traces, (geom.n_il, geom.n_xl, geom.n_t))
+        if vrms is None:
+            if not velocity > 0.0:
+                raise ValueError("a constant-velocity problem needs velocity > 0")
+            self.vrms, self.kind = None, 2
+        else:
+            v = _f32(vrms)
+            if v.ndim == 1:
+                if v.size != geom.n_t:
+                    raise ValueError("a Vrms trace has n_t samples")
+                self.vrms, self.kind = v, 1
+            else:
+                self.vrms, self.kind = _f32(v, (geom.n_il, geom.n_xl, geom.n_t)), 0
+        self.velocity = float(velocity)
+        self.out_center = np.ascontiguousarray(geom.out_center, dtype=np.int32)
+
+
+class Batch:
+    """Several problems (velocity-scan panels over one cube, sub-volumes with their own
+    Vrms) migrated by ONE persistent launch replayed as a CUDA graph (include/psm.h,
+    psm_batch_*).  The host arrays of the problems are kept referenced: reload() uploads
+    them again."""
+
+    PERSISTENT, PER_PROBLEM = 0, 1
+    DEPTH_FIRST, PROBLEM_ORDER = 0, 1
+    ORDERS = {0: "depth-first", 1: "problem"}
+
+    def __init__(self, migrator: "Migrator", problems):
+        self._m = migrator
+        self._L = migrator._L
+        self.problems = list(problems)
+        # a traces array shared by several problems must be the same object to share its
+        # device copy; _f32 keeps float32 C-contiguous inputs as they are
+        arr = (_lib.PsmProblem * len(self.problems))()
+        for i, p in enumerate(self.problems):
+            arr[i].geom = p.geom.to_c()
+            arr[i].out_center = p.out_center.ctypes.data
+            arr[i].traces = p.traces.ctypes.data
+            arr[i].vrms = p.vrms.ctypes.data if p.vrms is not None else None
+            arr[i].vrms_kind = p.kind
+            arr[i].velocity = p.velocity
+        self._arr = arr
+        self._b = ctypes.c_void_p()
+        check(self._L.psm_batch_create(migrator._ctx, arr, len(self.problems),
+                                       ctypes.byref(self._b)), migrator._err)
+
+    def close(self):
+        if self._b:
+            self._L.psm_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_mode(self, mode: int) -> None:
+        check(self._L.psm_batch_set_mode(self._b, int(mode)), self._m._err)
+
+    def set_variant(self, variant: int) -> None:
+        check(self._L.psm_batch_set_variant(self._b, int(variant)), self._m._err)
+
+    def variant(self) -> int:
+        v = ctypes.c_int()
+        check(self._L.psm_batch_get_variant(self._b, ctypes.byref(v)), self._m._err)
+        return v.value
+
+    def set_order(self, order: int) -> None:
+        check(self._L.psm_batch_set_order(self._b, int(order)), self._m._err)
+
+    def order(self) -> int:
+        o = ctypes.c_int()
+        check(self._L.psm_batch_get_order(self._b, ctypes.byref(o)), self._m._err)
+        return o.value
+
+    SCHEDULES = {0: "persistent/depth-first", 1: "persistent/problem", 2: "per-problem"}
+
+    def mode(self) -> int:
+        v = ctypes.c_int()
+        check(self._L.psm_batch_get_mode(self._b, ctypes.byref(v)), self._m._err)
+        return v.value
+
+    def autotune(self):
+        """Time every kernel variant on each schedule (persistent depth-first, persistent
+        problem order, per-problem launches); keep the fastest.
+        Returns (variant, order, mode, {(variant, schedule): ms})."""
+        nv = max(Migrator.VARIANTS) + 1
+        ms = np.zeros(3 * nv, dtype=np.float32)
+        best, order, mode = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._L.psm_batch_autotune(self._b, ms.ctypes.data, ctypes.byref(best),
+                                         ctypes.byref(order), ctypes.byref(mode)),
+              self._m._err)
+        return best.value, order.value, mode.value, {
+            (v, sch): float(ms[sch * nv + v]) for sch in (0, 1, 2) for v in Migrator.VARIANTS
+            if ms[sch * nv + v] > 0}
+
+    def reload(self) -> None:
+        check(self._L.psm_batch_reload(self._b), self._m._err)
+
+    def run_async(self) -> None:
+        check(self._L.psm_batch_run_async(self._b), self._m._err)
+
+    def synchronize(self) -> None:
+        check(self._L.psm_batch_synchronize(self._b), self._m._err)
+
+    def run(self) -> None:
+        check(self._L.psm_batch_run(self._b), self._m._err)
+
+    def image(self, i: int, out=None) -> np.ndarray:
+        g = self.problems[i].geom
+        shape = (g.n_oi, g.n_ox, g.n_t)
+        if out is None:
+            out = np.empty(shape, dtype=np.float32)
+        check(self._L.psm_batch_get_image(self._b, int(i), _addr(out)), self._m._err)
+        return out
+
+    def image_device_ptr(self, i: int) -> int:
+        p = ctypes.c_void_p()
+        check(self._L.psm_batch_image_device(self._b, int(i), ctypes.byref(p)), self._m._err)
+        return p.value
+
+    def count_terms(self) -> int:
+        n = ctypes.c_int64()
+        check(self._L.psm_batch_count_terms(self._b, ctypes.byref(n)), self._m._err)
+        return n.value
 
 
 class MigrationKernel:

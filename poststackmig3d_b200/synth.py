@@ -328,3 +328,32 @@ def random_workload(seed: int, n_il: int, n_xl: int, n_t: int, *, dt=0.004, d_il
         vel = 0.0
     return Workload(f"random{seed}", data, vr, vel, dt, d_il, d_xl, angle, amp, pad_il,
                     pad_xl, np.arange(10, 10 + n_il), np.arange(100, 100 + 2 * n_xl, 2))
+
+
+def workload_config4(seed: int = 4, n: int = 201, n_t: int = 751, n_panels: int = 32,
+                     n_sub: int = 8):
+    """Batched form: n_panels constant-velocity scan panels 1800 + 50 k m/s (k < 32, so
+    1800..3350) over one n x n x n_t cube (2 ms, 25 m bins, 20 diffractors + 3 dipping planes
+    modelled with Vrms 1800 -> 3400 m/s, 25 Hz Ricker, 5% noise), 30 deg aperture, amp on;
+    plus n_sub sub-volumes of 64-256 traces per axis and 401-1001 samples, each with its own
+    linear Vrms(t) (10 diffractors + 1 plane, 25 Hz, 5% noise).
+
+    Returns (panels, subvolumes): panels is a list of Workloads sharing one data array (the
+    velocity field differs), subvolumes a list of Workloads with Vrms cubes."""
+    vmod = linear_vrms(n, n, n_t, 0.002, 25.0, 1800.0, 3400.0, lateral=0.0)
+    data = reflectivity_cube(vmod, 0.002, 25.0, 20, 3, 25.0, 0.05, seed)
+    labels = np.arange(1, n + 1)
+    panels = [Workload(f"config4_panel{k}", data, None, 1800.0 + 50.0 * k, 0.002, 25.0, 25.0,
+                       30.0, True, 0, 0, labels, labels) for k in range(n_panels)]
+    rng = np.random.default_rng(seed + 1000)
+    subs = []
+    for k in range(n_sub):
+        ni, nx = (int(v) for v in rng.integers(64, 257, 2))
+        nt = int(rng.integers(401, 1002))
+        v0 = float(rng.uniform(1500.0, 2000.0))
+        v1 = float(rng.uniform(2500.0, 3500.0))
+        vr = linear_vrms(ni, nx, nt, 0.002, 25.0, v0, v1, lateral=0.0)
+        d = reflectivity_cube(vr, 0.002, 25.0, 10, 1, 25.0, 0.05, seed + 1 + k)
+        subs.append(Workload(f"config4_sub{k}", d, vr, 0.0, 0.002, 25.0, 25.0, 30.0, True, 0,
+                             0, np.arange(1, ni + 1), np.arange(1, nx + 1)))
+    return panels, subs
