@@ -34,6 +34,12 @@ class PsmProblem(ctypes.Structure):
                 ("vrms_kind", ctypes.c_int32), ("velocity", ctypes.c_float)]
 
 
+class PsmSlab(ctypes.Structure):
+    """Mirror of psm_slab (include/psm.h)."""
+    _fields_ = [("o0", ctypes.c_int32), ("o1", ctypes.c_int32), ("i0", ctypes.c_int32),
+                ("i1", ctypes.c_int32)]
+
+
 class PsmError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS.get(code, code)}: {msg}")
@@ -61,6 +67,15 @@ _CUDA_SYMBOLS = [
     ("psm_stream", ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     ("psm_count_terms", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     ("psm_count_terms_rows", ctypes.c_int, [_P, _P]),
+    ("psm_slab_bytes", ctypes.c_int64, [ctypes.POINTER(PsmGeom), ctypes.c_int32,
+                                        ctypes.c_int32]),
+    ("psm_plan_slabs", ctypes.c_int, [ctypes.POINTER(PsmGeom), _P, ctypes.c_int64, _P,
+                                      ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    ("psm_split_slabs", ctypes.c_int, [ctypes.POINTER(PsmGeom), _P, _P, ctypes.c_int32, _P]),
+    ("psm_slab_geometry", ctypes.c_int, [ctypes.POINTER(PsmGeom), _P, _P,
+                                         ctypes.POINTER(PsmGeom), _P]),
+    ("psm_forward_streamed", ctypes.c_int, [_P, ctypes.POINTER(PsmGeom), _P, _P, _P, _P,
+                                            ctypes.c_int64]),
     ("psm_set_vrms_table", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int32, _P, _P]),
     ("psm_set_vrms_grid", ctypes.c_int, [_P, _P, _P, ctypes.c_int32, _P, ctypes.c_int32,
                                          ctypes.c_int32, ctypes.c_double, _P, _P]),

@@ -144,6 +144,57 @@ def plan_geometry(n_il: int, n_xl: int, n_t: int, dt_seconds: float, d_il: float
                     output_centers(il_labels, out_il), amp, precision)
 
 
+# ----------------------------------------------------------------------------- slabs
+
+Slab = tuple  # (o0, o1, i0, i1): output inlines [o0, o1) read input inlines [i0, i1)
+
+
+def _slab_tuple(s) -> Slab:
+    return (s.o0, s.o1, s.i0, s.i1)
+
+
+def slab_bytes(g: Geometry, n_in: int, n_out: int) -> int:
+    """Device bytes a slab of n_in input and n_out output inlines holds (psm_slab_bytes)."""
+    gc = g.to_c()
+    return int(_lib.cuda().psm_slab_bytes(ctypes.byref(gc), int(n_in), int(n_out)))
+
+
+def plan_slabs(g: Geometry, max_device_bytes: int):
+    """Consecutive slabs of output inlines of at most max_device_bytes each."""
+    gc = g.to_c()
+    oc = np.ascontiguousarray(g.out_center, dtype=np.int32)
+    arr = (_lib.PsmSlab * max(g.n_oi, 1))()
+    n = ctypes.c_int32()
+    check(_lib.cuda().psm_plan_slabs(ctypes.byref(gc), oc.ctypes.data, int(max_device_bytes),
+                                     arr, g.n_oi, ctypes.byref(n)), lambda: "psm_plan_slabs")
+    return [_slab_tuple(arr[k]) for k in range(n.value)]
+
+
+def split_slabs(g: Geometry, n_parts: int, weight=None):
+    """n_parts consecutive slabs of about equal work (weight[o] per output inline)."""
+    gc = g.to_c()
+    oc = np.ascontiguousarray(g.out_center, dtype=np.int32)
+    w = None if weight is None else np.ascontiguousarray(weight, dtype=np.float64)
+    arr = (_lib.PsmSlab * n_parts)()
+    check(_lib.cuda().psm_split_slabs(ctypes.byref(gc), oc.ctypes.data,
+                                      None if w is None else w.ctypes.data, int(n_parts), arr),
+          lambda: "psm_split_slabs")
+    return [_slab_tuple(arr[k]) for k in range(n_parts)]
+
+
+def slab_geometry(g: Geometry, slab: Slab) -> Geometry:
+    """The slab as a problem of its own (traces and Vrms from input inline slab[2] on)."""
+    gc = g.to_c()
+    oc = np.ascontiguousarray(g.out_center, dtype=np.int32)
+    s = _lib.PsmSlab(*slab)
+    loc = PsmGeom()
+    lc = np.zeros(max(slab[1] - slab[0], 1), dtype=np.int32)
+    check(_lib.cuda().psm_slab_geometry(ctypes.byref(gc), oc.ctypes.data, ctypes.byref(s),
+                                        ctypes.byref(loc), lc.ctypes.data),
+          lambda: "psm_slab_geometry")
+    return dataclasses.replace(g, n_il=loc.n_il, n_oi=loc.n_oi, out_center=lc[:loc.n_oi])
+
+
 def estimate_max_velocity(vrms: np.ndarray) -> float:
     """src/main.cpp:22-64 on a dense Vrms cube: max over (first, middle, last) inline x
     (first, middle, last) crossline at the last sample; below 100 m/s -> 3000."""
@@ -201,6 +252,20 @@ class Migrator:
         if isinstance(data, np.ndarray):
             data = _f32(data, (g.n_il, g.n_xl, g.n_t))
         check(self._L.psm_set_traces(self._ctx, _addr(data)), self._err)
+
+    def forward_streamed(self, g: Geometry, traces, vrms, max_device_bytes: int) -> np.ndarray:
+        """Migrate a host-resident cube in slabs of at most max_device_bytes of device memory
+        (psm_forward_streamed); the ctx's geometry is the last slab's afterwards."""
+        tr = _f32(traces, (g.n_il, g.n_xl, g.n_t))
+        vr = _f32(vrms, (g.n_il, g.n_xl, g.n_t))
+        img = np.empty((g.n_oi, g.n_ox, g.n_t), dtype=np.float32)
+        gc = g.to_c()
+        oc = np.ascontiguousarray(g.out_center, dtype=np.int32)
+        check(self._L.psm_forward_streamed(self._ctx, ctypes.byref(gc), oc.ctypes.data,
+                                           tr.ctypes.data, vr.ctypes.data, img.ctypes.data,
+                                           int(max_device_bytes)), self._err)
+        self.geom = None
+        return img
 
     def set_vrms_table(self, points, il_labels, xl_labels) -> None:
         """Vrms from a text table's points [(il, xl, time_s, v), ...], assembled on the GPU."""
