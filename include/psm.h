@@ -207,7 +207,7 @@ int psm_adjoint(psm_ctx *ctx, const float *image, float *data);
 int psm_lsm_cg(psm_ctx *ctx, const float *data, float *image, int iters, double *resid);
 
 /* Forward-kernel variants: f32x2-packed or scalar FP32 arithmetic for each pair of 32-sample
- * blocks, 2 or 4 blocks behind one warp-uniform skip test, and 8 or 16 blocks per lane (a
+ * blocks, 2, 4 or 8 blocks behind one warp-uniform skip test, and 8 or 16 blocks per lane (a
  * tile of 256 or 512 output samples).  All give the same masks and the same terms, bit for
  * bit; they differ in instruction count and shared-memory traffic.  PSM_FWD_DEFAULT lets the
  * library pick (the result of psm_autotune once it has run on the ctx). */
@@ -219,7 +219,11 @@ typedef enum {
     PSM_FWD_PACKED_G4 = 4,
     PSM_FWD_PACKED_G4_J16 = 5,
     PSM_FWD_SCALAR_G4_J16 = 6,
-    PSM_FWD_N_VARIANTS = 7
+    PSM_FWD_PACKED_G8 = 7,
+    PSM_FWD_SCALAR_G8 = 8,
+    PSM_FWD_PACKED_G4_O3 = 9,  /* 3 CTAs per SM: 72 registers, 32 KB stages */
+    PSM_FWD_SCALAR_G4_O3 = 10,
+    PSM_FWD_N_VARIANTS = 11
 } psm_fwd_variant;
 int psm_set_variant(psm_ctx *ctx, int variant);
 int psm_get_variant(psm_ctx *ctx, int *variant);

@@ -90,27 +90,49 @@ size_t fwd_smem(const FwdParams& P, int store = psm::kStoreF32) {
     return b <= kMaxDynSmem ? b : 0;
 }
 
-constexpr int kDefaultVariant = PSM_FWD_PACKED_G4;
+constexpr int kDefaultVariant = PSM_FWD_PACKED_G4_O3;
 
 inline bool is_j16(int variant) {
     return variant == PSM_FWD_PACKED_G4_J16 || variant == PSM_FWD_SCALAR_G4_J16;
 }
 
-// The variant that actually runs: 16-bit storage runs the packed skip-4 kernel with the
-// variant's blocks per lane, compensated summation the packed skip-4 kernel with 8 (its
-// partial and compensation registers leave no room for 16).
+inline bool is_o3(int variant) {
+    return variant == PSM_FWD_PACKED_G4_O3 || variant == PSM_FWD_SCALAR_G4_O3;
+}
+
+// The variant that actually runs: 16-bit storage and compensated summation run the packed
+// skip-4 kernel, with 16 blocks a lane (16-bit storage only: compensation's partial and
+// compensation registers leave no room for 16), or built for 3 CTAs per SM, or else the
+// default build.
 inline int effective_variant(int variant, int store, bool kahan) {
     if (variant == PSM_FWD_DEFAULT) variant = kDefaultVariant;
     if (store == psm::kStoreF32 && !kahan) return variant;
-    return !kahan && is_j16(variant) ? PSM_FWD_PACKED_G4_J16 : PSM_FWD_PACKED_G4;
+    if (!kahan && is_j16(variant)) return PSM_FWD_PACKED_G4_J16;
+    return is_o3(variant) ? PSM_FWD_PACKED_G4_O3 : PSM_FWD_PACKED_G4;
 }
 
-// One instantiation of the forward kernel templates.
-template <bool AMP_, bool PACKED_, int GB_, int J_, int STORE_, bool KAHAN_>
+// One instantiation of the forward kernel templates (MINB: CTAs per SM the kernel is built
+// for, 2 or 3).
+template <bool AMP_, bool PACKED_, int GB_, int J_, int STORE_, bool KAHAN_, int MINB_ = 2>
 struct KernelTag {
     static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_;
-    static constexpr int GB = GB_, J = J_, STORE = STORE_;
+    static constexpr int GB = GB_, J = J_, STORE = STORE_, MINB = MINB_;
 };
+
+// Samples per stage of the kernel built for 3 CTAs per SM (32 KB), so that its shared memory
+// fits the SM three times.
+inline int stage_cap_for(int minb, int store) {
+    const int bytes = minb == 3 ? 32768 : 8 * psm::kStageCapMin;
+    return bytes / psm::store_bytes(store);
+}
+
+template <class K>
+auto grid_kernel() {
+    if constexpr (K::MINB == 3)
+        return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+    else
+        return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+}
 
 // Calls f(KernelTag<...>{}) for the kernel that (amp, effective variant, store, kahan) names.
 template <bool AMP, class F>
@@ -118,7 +140,7 @@ cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
     using psm::kStoreBF16;
     using psm::kStoreF16;
     using psm::kStoreF32;
-    const bool j16 = is_j16(variant);
+    const bool j16 = is_j16(variant), o3 = is_o3(variant);
     switch (store * 2 + (kahan ? 1 : 0)) {
         case kStoreF32 * 2:
             switch (variant) {
@@ -130,17 +152,32 @@ cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
                     return f(KernelTag<AMP, true, 4, 16, kStoreF32, false>{});
                 case PSM_FWD_SCALAR_G4_J16:
                     return f(KernelTag<AMP, false, 4, 16, kStoreF32, false>{});
+                case PSM_FWD_PACKED_G8: return f(KernelTag<AMP, true, 8, 8, kStoreF32, false>{});
+                case PSM_FWD_SCALAR_G8: return f(KernelTag<AMP, false, 8, 8, kStoreF32, false>{});
+                case PSM_FWD_PACKED_G4_O3:
+                    return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3>{});
+                case PSM_FWD_SCALAR_G4_O3:
+                    return f(KernelTag<AMP, false, 4, 8, kStoreF32, false, 3>{});
+
                 default: return cudaErrorInvalidValue;
             }
-        case kStoreF32 * 2 + 1: return f(KernelTag<AMP, true, 4, 8, kStoreF32, true>{});
+        case kStoreF32 * 2 + 1:
+            return o3 ? f(KernelTag<AMP, true, 4, 8, kStoreF32, true, 3>{})
+                      : f(KernelTag<AMP, true, 4, 8, kStoreF32, true>{});
         case kStoreBF16 * 2:
-            return j16 ? f(KernelTag<AMP, true, 4, 16, kStoreBF16, false>{})
-                       : f(KernelTag<AMP, true, 4, 8, kStoreBF16, false>{});
-        case kStoreBF16 * 2 + 1: return f(KernelTag<AMP, true, 4, 8, kStoreBF16, true>{});
+            return j16  ? f(KernelTag<AMP, true, 4, 16, kStoreBF16, false>{})
+                   : o3 ? f(KernelTag<AMP, true, 4, 8, kStoreBF16, false, 3>{})
+                        : f(KernelTag<AMP, true, 4, 8, kStoreBF16, false>{});
+        case kStoreBF16 * 2 + 1:
+            return o3 ? f(KernelTag<AMP, true, 4, 8, kStoreBF16, true, 3>{})
+                      : f(KernelTag<AMP, true, 4, 8, kStoreBF16, true>{});
         case kStoreF16 * 2:
-            return j16 ? f(KernelTag<AMP, true, 4, 16, kStoreF16, false>{})
-                       : f(KernelTag<AMP, true, 4, 8, kStoreF16, false>{});
-        case kStoreF16 * 2 + 1: return f(KernelTag<AMP, true, 4, 8, kStoreF16, true>{});
+            return j16  ? f(KernelTag<AMP, true, 4, 16, kStoreF16, false>{})
+                   : o3 ? f(KernelTag<AMP, true, 4, 8, kStoreF16, false, 3>{})
+                        : f(KernelTag<AMP, true, 4, 8, kStoreF16, false>{});
+        case kStoreF16 * 2 + 1:
+            return o3 ? f(KernelTag<AMP, true, 4, 8, kStoreF16, true, 3>{})
+                      : f(KernelTag<AMP, true, 4, 8, kStoreF16, true>{});
         default: return cudaErrorInvalidValue;
     }
 }
@@ -156,15 +193,19 @@ cudaError_t with_kernel(bool amp, int variant, int store, bool kahan, F&& f) {
 // to the kernel, so it must cover the largest launch of the capture).
 template <class K>
 cudaError_t prepare_grid(K, size_t smem) {
-    return cudaFuncSetAttribute(psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(grid_kernel<K>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem));
 }
 
 template <class K>
-cudaError_t launch_grid(K, const FwdParams& P, int n_jobs, size_t smem, cudaStream_t s) {
+cudaError_t launch_grid(K, const FwdParams& P_in, int n_jobs, size_t smem, cudaStream_t s) {
     constexpr int TT = 32 * K::J;
-    auto* kern = psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+    auto* kern = grid_kernel<K>();
+    FwdParams P = P_in;
+    if constexpr (K::MINB > 2) {  // smaller stages, so that MINB CTAs fit an SM
+        P.stage_cap = std::max(stage_cap_for(K::MINB, K::STORE), P.ns);
+        smem = std::min(smem, fwd_smem(P, K::STORE));
+    }
     dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + TT - 1) / TT, n_jobs);
     dim3 block(32 * (psm::kTX + 1));
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;

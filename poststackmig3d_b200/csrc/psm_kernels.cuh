@@ -525,7 +525,7 @@ __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2
 }
 
 // Kernel variants: PACKED selects f32x2 or scalar FP32 arithmetic for a block pair; GB is
-// the number of 32-sample blocks behind one warp-uniform skip test (2 or 4); J the number
+// the number of 32-sample blocks behind one warp-uniform skip test (2, 4 or 8); J the number
 // of 32-sample blocks per lane (the tile covers 32 J output samples).  STORE is the trace
 // storage (kStoreF32 pairs, or 16-bit words with a per-trace scale; 16-bit storage always
 // uses the packed arithmetic).  KAHAN adds compensated summation: each ring stage (at most
@@ -542,7 +542,7 @@ template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN>
 __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int x0, int T0,
                                          unsigned char* smem_raw, const SmemLayout& L,
                                          uint32_t& it) {
-    static_assert(GB == 2 || GB == 4, "skip groups of 2 or 4 blocks");
+    static_assert(GB == 2 || GB == 4 || GB == 8, "skip groups of 2, 4 or 8 blocks");
     static_assert(J % GB == 0, "whole skip groups per lane");
     static_assert(STORE == kStoreF32 || PACKED, "16-bit storage uses packed arithmetic");
     constexpr int NG = J / GB;   // skip groups per lane
@@ -927,6 +927,18 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);  // ordered by the tile's first barrier
+    uint32_t it = 0;
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
+                                               blockIdx.y * 32 * J, smem_raw, L, it);
+}
+
+// The same with 3 CTAs per SM (27 warps): registers are held to 72 per thread and the launcher
+// gives it stages of 32 KB, so that three CTAs fit the SM's registers and shared memory.
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false>
+__global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdParams P) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
+    if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
     fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
                                                blockIdx.y * 32 * J, smem_raw, L, it);
