@@ -209,7 +209,10 @@ int psm_lsm_cg(psm_ctx *ctx, const float *data, float *image, int iters, double 
 /* Forward-kernel variants: f32x2-packed or scalar FP32 arithmetic for each pair of 32-sample
  * blocks, 2, 4 or 8 blocks behind one warp-uniform skip test, and 8 or 16 blocks per lane (a
  * tile of 256 or 512 output samples).  All give the same masks and the same terms, bit for
- * bit; they differ in instruction count and shared-memory traffic.  PSM_FWD_DEFAULT lets the
+ * bit; they differ in instruction count and shared-memory traffic.  The PAIRS variants (fp32
+ * storage) evaluate the travel time once for the two traces at inlines c - d and c + d of one
+ * crossline, which share it, and add their two samples before the weight: the same terms,
+ * summed in another order (equal to FP32 rounding).  PSM_FWD_DEFAULT lets the
  * library pick (the result of psm_autotune once it has run on the ctx). */
 typedef enum {
     PSM_FWD_DEFAULT = 0,
@@ -223,7 +226,9 @@ typedef enum {
     PSM_FWD_SCALAR_G8 = 8,
     PSM_FWD_PACKED_G4_O3 = 9,  /* 3 CTAs per SM: 72 registers, 32 KB stages */
     PSM_FWD_SCALAR_G4_O3 = 10,
-    PSM_FWD_N_VARIANTS = 11
+    PSM_FWD_PAIRS_O3 = 11, /* mirrored inlines c - d, c + d staged as pairs, 3 CTAs per SM */
+    PSM_FWD_PAIRS = 12,
+    PSM_FWD_N_VARIANTS = 13
 } psm_fwd_variant;
 int psm_set_variant(psm_ctx *ctx, int variant);
 int psm_get_variant(psm_ctx *ctx, int *variant);

@@ -90,14 +90,15 @@ size_t fwd_smem(const FwdParams& P, int store = psm::kStoreF32) {
     return b <= kMaxDynSmem ? b : 0;
 }
 
-constexpr int kDefaultVariant = PSM_FWD_PACKED_G4_O3;
+constexpr int kDefaultVariant = PSM_FWD_PAIRS_O3;
 
 inline bool is_j16(int variant) {
     return variant == PSM_FWD_PACKED_G4_J16 || variant == PSM_FWD_SCALAR_G4_J16;
 }
 
 inline bool is_o3(int variant) {
-    return variant == PSM_FWD_PACKED_G4_O3 || variant == PSM_FWD_SCALAR_G4_O3;
+    return variant == PSM_FWD_PACKED_G4_O3 || variant == PSM_FWD_SCALAR_G4_O3 ||
+           variant == PSM_FWD_PAIRS_O3;
 }
 
 // The variant that actually runs: 16-bit storage and compensated summation run the packed
@@ -113,9 +114,10 @@ inline int effective_variant(int variant, int store, bool kahan) {
 
 // One instantiation of the forward kernel templates (MINB: CTAs per SM the kernel is built
 // for, 2 or 3).
-template <bool AMP_, bool PACKED_, int GB_, int J_, int STORE_, bool KAHAN_, int MINB_ = 2>
+template <bool AMP_, bool PACKED_, int GB_, int J_, int STORE_, bool KAHAN_, int MINB_ = 2,
+          bool PAIRS_ = false>
 struct KernelTag {
-    static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_;
+    static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_, PAIRS = PAIRS_;
     static constexpr int GB = GB_, J = J_, STORE = STORE_, MINB = MINB_;
 };
 
@@ -129,9 +131,9 @@ inline int stage_cap_for(int minb, int store) {
 template <class K>
 auto grid_kernel() {
     if constexpr (K::MINB == 3)
-        return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+        return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
     else
-        return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+        return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
 }
 
 // Calls f(KernelTag<...>{}) for the kernel that (amp, effective variant, store, kahan) names.
@@ -158,6 +160,9 @@ cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
                     return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3>{});
                 case PSM_FWD_SCALAR_G4_O3:
                     return f(KernelTag<AMP, false, 4, 8, kStoreF32, false, 3>{});
+                case PSM_FWD_PAIRS_O3:
+                    return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3, true>{});
+                case PSM_FWD_PAIRS: return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 2, true>{});
 
                 default: return cudaErrorInvalidValue;
             }
@@ -264,6 +269,7 @@ void fill_consts(FwdParams& P, float dt, float d_il, float d_xl, float tan2) {
     P.ntm1m = std::nextafter(P.ntm1f, 0.0f);
     P.vs_x = P.n_t;  // dense Vrms cube [n_vrow][n_vx][n_t]
     P.vs_row = static_cast<long long>(P.n_vx) * P.n_t;
+    P.pairable = 1;  // inline positions 0, 1, 2, ... (the per-inline drop-in checks its own)
 }
 
 // Argument checks of a geometry: PSM_OK, or the status with *why set.
@@ -1261,7 +1267,7 @@ namespace {
 // kernel K; done before a stream capture, so the graph holds only the launch.
 template <class K>
 cudaError_t prepare_persistent(K, psm_batch& b) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
     const size_t smem =
         psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1279,7 +1285,7 @@ cudaError_t prepare_persistent(K, psm_batch& b) {
 
 template <class K>
 cudaError_t launch_persistent(K, const psm_batch& b, cudaStream_t s) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN>;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
     const size_t smem =
         psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
     const int w = (K::J == 16 ? 2 : 0) + b.order;
@@ -1850,6 +1856,8 @@ int psm_kirchhoff_inline(const float* input_buffer, size_t n_buf_il, size_t n_bu
     P.max_inl = std::max<int>(static_cast<int>(n_buf_il), 1);
     P.stage_cap = stage_cap(ns);
     fill_consts(P, dt, inline_bin_size, crossline_bin_size, tan_theta_sq);
+    for (size_t i = 1; i < n_buf_il; ++i)  // mirrored pairs need consecutive inline positions
+        if (il_pos_indices[i] != il_pos_indices[i - 1] + 1) P.pairable = 0;
     PSM_INL_TRY(launch_fwd(P, 1, amp_correction != 0, PSM_FWD_DEFAULT, s));
     PSM_INL_TRY(cudaMemcpyAsync(output_slice, S->out.p, n_out_xl * n_t * sizeof(float),
                                 cudaMemcpyDeviceToHost, s));

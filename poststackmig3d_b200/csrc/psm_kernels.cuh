@@ -82,6 +82,7 @@ struct FwdParams {
     int xoff;             // cube / Vrms crossline of output x is x + xoff
     int max_inl;          // largest i1 - i0 over the jobs (inline-table capacity)
     int stage_cap;        // samples per ring stage (of store_bytes each)
+    int pairable;         // il_pos consecutive: mirrored inlines c - d, c + d can be paired
     float inv_dt, idt2, d_il, d_xl, inv_dxl, tan2, tanth;
     float ntm1f;          // n_t - 1
     float ntm1m;          // largest float below n_t - 1
@@ -95,6 +96,9 @@ struct StageMeta {
     float shi[kMaxG]; // largest s that stays inside the window
     float sc[kMaxG];  // trace scale (16-bit storage)
     float wend[kMaxG];  // window end as float (read by the debug-bounds build)
+    int baseb[kMaxG];   // paired slots: window base of the mirrored trace (see consumers)
+    unsigned pairmask;  // bit g: slot g holds a mirrored pair of traces
+    int pad2[3];
 };
 
 struct TileStats {
@@ -353,6 +357,24 @@ __global__ void quantize_kernel(const float* __restrict__ src, uint32_t* __restr
 
 // ----------------------------------------------------------------------------- forward
 
+// Buffer inlines (local indices) of row r of the producer's trace list: with pc < 0 the row is
+// inline r; else row r is the mirror distance from the centre inline pc, holding inlines
+// pc - r and pc + r (*b = -1 when the row has one inline: r = 0, or one side outside the
+// buffer).
+__device__ __forceinline__ void row_inlines(int pc, int n_inl, int r, int* a, int* b) {
+    if (pc < 0) {
+        *a = r;
+        *b = -1;
+        return;
+    }
+    *a = pc - r;
+    *b = r > 0 && pc + r < n_inl ? pc + r : -1;
+    if (*a < 0) {
+        *a = pc + r;
+        *b = -1;
+    }
+}
+
 // Producer: lo of every passing term of the tile on trace (dx2, kc) lies in [*lolo, *lohi]
 // (with two samples of slack for rounding); false when the trace has no passing term.
 // Bounds: t >= t0 and, inside the aperture r <= v t0 tan/2, t0 >= 2 r_min / (v_max tan);
@@ -483,6 +505,38 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
         ACC = add2(ACC, make_float2(v0, v1));
 }
 
+// Block pair of a mirrored pair of staged traces (inlines c - d and c + d at one crossline:
+// the same r^2, so the same travel times, sample indices, fractions and weights).  The two
+// interpolated values are added before the weight; each trace's window has its own base.
+template <bool AMP, bool MASK>
+__device__ __forceinline__ void term_pair2(const unsigned char* sbase, float r2, uint32_t base2a,
+                                           uint32_t base2b, const Win& w, const float2& T2,
+                                           const float2& F4, const float2& BB, float2& ACC) {
+    const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
+    const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
+    float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
+    s.x = window_s<MASK>(s.x, w);                            // inside the staged windows
+    s.y = window_s<MASK>(s.y, w);
+    const float2 M = make_float2(8388608.0f, 8388608.0f);
+    const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
+    const float2 fr = sub2(s, sub2(mm, M));                  // frac
+    const uint32_t o0 = __float_as_uint(mm.x) << 3, o1 = __float_as_uint(mm.y) << 3;
+    const float2 a0 = *reinterpret_cast<const float2*>(sbase + (base2a + o0));
+    const float2 a1 = *reinterpret_cast<const float2*>(sbase + (base2a + o1));
+    const float2 b0 = *reinterpret_cast<const float2*>(sbase + (base2b + o0));
+    const float2 b1 = *reinterpret_cast<const float2*>(sbase + (base2b + o1));
+    float2 v = add2(make_float2(fmaf(fr.x, a0.y, a0.x), fmaf(fr.y, a1.y, a1.x)),
+                    make_float2(fmaf(fr.x, b0.y, b0.x), fmaf(fr.y, b1.y, b1.x)));
+    if (MASK) {
+        v.x = r2 <= BB.x ? v.x : 0.0f;
+        v.y = r2 <= BB.y ? v.y : 0.0f;
+    }
+    if (AMP)
+        ACC = fma2(v, make_float2(q0, q1), ACC);
+    else
+        ACC = add2(ACC, v);
+}
+
 // Both samples of a 16-bit storage word as fp32 (exact conversions).
 template <int STORE>
 __device__ __forceinline__ float2 unpack16(uint32_t w) {
@@ -524,6 +578,57 @@ __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2
         ACC = fma2(v, make_float2(sc, sc), ACC);
 }
 
+// One block pair of a staged slot: a single trace (fp32 or 16-bit storage) or a mirrored pair.
+template <bool AMP, bool MASK, bool PACKED, int STORE, bool TWO>
+__device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2, uint32_t base2,
+                                          uint32_t base2b, const Win& w, float sc,
+                                          const float2& T2, const float2& F4, const float2& BB,
+                                          float2& ACC) {
+    if (TWO)
+        term_pair2<AMP, MASK>(sbase, r2, base2, base2b, w, T2, F4, BB, ACC);
+    else if (STORE == kStoreF32)
+        term_pair<AMP, MASK, PACKED>(sbase, r2, base2, w, T2, F4, BB, ACC);
+    else
+        term_pair16<AMP, MASK, STORE>(sbase, r2, base2, w, sc, T2, F4, BB, ACC);
+}
+
+// One staged slot for one consumer warp: every block pair of the lane where some lane of its
+// group passes, without masks where every lane of the group (or of the tile) passes.
+template <bool AMP, bool PACKED, int GB, int J, int STORE, bool TWO>
+__device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2, uint32_t base2,
+                                           uint32_t base2b, Win w, const float* shi, float sc,
+                                           float gminall, const float (&gmax)[J / GB],
+                                           const float (&gmin)[J / GB], const float2 (&T2)[J / 2],
+                                           const float2 (&F4)[J / 2], const float2 (&BB)[J / 2],
+                                           float2 (&SUM)[J / 2]) {
+    constexpr int NG = J / GB;
+    constexpr int PG = GB / 2;
+    if (r2 <= gminall) {  // interior trace: every term of the tile passes
+#pragma unroll
+        for (int p = 0; p < J / 2; ++p)
+            eval_pair<AMP, false, PACKED, STORE, TWO>(sbase, r2, base2, base2b, w, sc, T2[p],
+                                                      F4[p], BB[p], SUM[p]);
+        return;
+    }
+    w.shi = *shi;
+#pragma unroll
+    for (int gr = 0; gr < NG; ++gr) {
+        if (r2 <= gmax[gr]) {
+            if (r2 <= gmin[gr]) {  // every lane of the group passes
+#pragma unroll
+                for (int p = PG * gr; p < PG * (gr + 1); ++p)
+                    eval_pair<AMP, false, PACKED, STORE, TWO>(sbase, r2, base2, base2b, w, sc,
+                                                              T2[p], F4[p], BB[p], SUM[p]);
+            } else {
+#pragma unroll
+                for (int p = PG * gr; p < PG * (gr + 1); ++p)
+                    eval_pair<AMP, true, PACKED, STORE, TWO>(sbase, r2, base2, base2b, w, sc,
+                                                             T2[p], F4[p], BB[p], SUM[p]);
+            }
+        }
+    }
+}
+
 // Kernel variants: PACKED selects f32x2 or scalar FP32 arithmetic for a block pair; GB is
 // the number of 32-sample blocks behind one warp-uniform skip test (2, 4 or 8); J the number
 // of 32-sample blocks per lane (the tile covers 32 J output samples).  STORE is the trace
@@ -538,15 +643,15 @@ __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2
 // per CTA (ring_init); it counts the ring stages the CTA has used so far, so consecutive tiles
 // of a persistent CTA continue the ring's phases (every stage, the end-of-stream marker
 // included, is released by the consumers).  Returns false when a bounded wait expired.
-template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN>
+template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false>
 __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int x0, int T0,
                                          unsigned char* smem_raw, const SmemLayout& L,
                                          uint32_t& it) {
     static_assert(GB == 2 || GB == 4 || GB == 8, "skip groups of 2, 4 or 8 blocks");
     static_assert(J % GB == 0, "whole skip groups per lane");
     static_assert(STORE == kStoreF32 || PACKED, "16-bit storage uses packed arithmetic");
+    static_assert(!PAIRS || (STORE == kStoreF32 && PACKED), "mirrored pairs: packed fp32");
     constexpr int NG = J / GB;   // skip groups per lane
-    constexpr int PG = GB / 2;   // block pairs per group
     constexpr int EB = store_bytes(STORE);
     // bits(2^23) << log2(EB), modulo 2^32 (see the producer)
     constexpr uint32_t MAGIC = EB == 8 ? 0x58000000u : 0x2C000000u;
@@ -666,15 +771,26 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         int* inl_pre = reinterpret_cast<int*>(smem_raw + L.inl_pre);
         float* inl_dx2 = reinterpret_cast<float*>(smem_raw + L.inl_dx2);
         const int n_inl = max(job.i1 - job.i0, 0);
+        // rows of the trace list: the buffer inlines, or (PAIRS) the mirror distances d from the
+        // centre inline pc, row d holding inlines pc - d and pc + d, whose traces at one
+        // crossline have the same r^2 to every output point
+        int pc = -1;  // pairs need two whole windows in one stage (a window is at most ns)
+        if (PAIRS && P.pairable && 2 * P.ns <= P.stage_cap && n_inl > 0) {
+            const int c = job.pos - __ldg(P.il_pos + job.i0);
+            if (c >= 0 && c < n_inl) pc = c;
+        }
+        const int n_rows = pc >= 0 ? max(pc, n_inl - 1 - pc) + 1 : n_inl;
         int total = 0;
         if (S.any && xa <= xb) {
-            // inline table: crossline range and running trace count per buffer inline
-            for (int base = 0; base < n_inl; base += 32) {
+            // row table: crossline range and running slot count per row
+            for (int base = 0; base < n_rows; base += 32) {
                 const int n = base + lane;
                 int cnt = 0, klo = 0;
                 float dx2 = 0.0f;
-                if (n < n_inl) {
-                    dx2 = inline_dx2(__ldg(P.il_pos + job.i0 + n), job.pos, P.d_il);
+                if (n < n_rows) {
+                    int a, b;
+                    row_inlines(pc, n_inl, n, &a, &b);
+                    dx2 = inline_dx2(__ldg(P.il_pos + job.i0 + a), job.pos, P.d_il);
                     if (dx2 <= S.bmax) {
                         const int K =
                             static_cast<int>(sqrtf(fmaxf(S.bmax - dx2, 0.0f)) * P.inv_dxl) + 2;
@@ -690,21 +806,21 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     const int v = __shfl_up_sync(0xffffffffu, incl, o);
                     if (lane >= o) incl += v;
                 }
-                if (n < n_inl) inl_pre[n] = total + incl - cnt;
+                if (n < n_rows) inl_pre[n] = total + incl - cnt;
                 total += __shfl_sync(0xffffffffu, incl, 31);
             }
-            if (lane == 0) inl_pre[n_inl] = total;
+            if (lane == 0) inl_pre[n_rows] = total;
             __syncwarp();
         }
         bool alive = true;
         int f = 0;
         while (f < total && alive) {
             const int idx = f + lane;
-            int ws = 0, size = 0, kc = 0, row = 0;
+            int ws = 0, size = 0, kc = 0, row = 0, rowb = -1, slot_size = 0;
             float dx2 = 0.0f, shi = 0.0f, sc = 1.0f;
             if (idx < total) {
-                // buffer inline of flat trace idx: the last n with inl_pre[n] <= idx
-                int lo = 0, hi = n_inl - 1;
+                // row of flat slot idx: the last n with inl_pre[n] <= idx
+                int lo = 0, hi = n_rows - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
                     if (inl_pre[mid] <= idx)
@@ -714,13 +830,17 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                 }
                 kc = inl_klo[lo] + (idx - inl_pre[lo]);
                 dx2 = inl_dx2[lo];
-                row = job.i0 + lo;
+                int a, b;
+                row_inlines(pc, n_inl, lo, &a, &b);
+                row = job.i0 + a;
+                rowb = b >= 0 ? job.i0 + b : -1;
                 trace_window<STORE>(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
                 if (STORE != kStoreF32 && size > 0)
                     sc = __ldg(P.scales + static_cast<size_t>(row) * P.n_cx + kc);
+                slot_size = rowb >= 0 ? 2 * size : size;  // a pair's windows are the same
             }
-            // inclusive prefix sum of window sizes; take the lanes that fit one stage
-            int cum = size;
+            // inclusive prefix sum of slot sizes; take the lanes that fit one stage
+            int cum = slot_size;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int v = __shfl_up_sync(0xffffffffu, cum, o);
@@ -742,10 +862,13 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                 StageMeta& m = meta[stage];
                 const int tot = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
                 const uint32_t dst_rel =
-                    L.stage + (static_cast<uint32_t>(stage) * P.stage_cap + (cum - size)) * EB;
+                    L.stage +
+                    (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) * EB;
                 const uint32_t dst = stage0 + (dst_rel - L.stage);
+                const int slot = __popc(nzmask & ((1u << lane) - 1u));
+                const unsigned pm = __reduce_or_sync(
+                    0xffffffffu, take && size > 0 && rowb >= 0 ? (1u << slot) : 0u);
                 if (take && size > 0) {
-                    const int slot = __popc(nzmask & ((1u << lane) - 1u));
                     // consumers find sample n of the window at byte
                     // base2 + (bits(2^23 + n) << log2(EB)) from the shared-memory base (32-bit
                     // wrap-around): base2 = dst_rel - EB ws - (0x4B000000 << log2(EB))
@@ -755,8 +878,12 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     m.shi[slot] = shi;
                     m.sc[slot] = sc;
                     m.wend[slot] = static_cast<float>(ws + size);
+                    m.baseb[slot] = static_cast<int>(dst_rel + EB * size - EB * ws - MAGIC);
                 }
-                if (lane == 0) m.count = n;
+                if (lane == 0) {
+                    m.count = n;
+                    m.pairmask = pm;
+                }
                 __threadfence_block();
                 __syncwarp();
                 if (lane == 0)
@@ -768,6 +895,11 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                                           ? static_cast<const void*>(P.pairs + off)
                                           : static_cast<const void*>(P.words + off);
                     tma_load_1d(dst, src, static_cast<uint32_t>(size) * EB, &full[stage]);
+                    if (rowb >= 0) {  // the mirrored trace's window right after
+                        const size_t offb = (static_cast<size_t>(rowb) * P.n_cx + kc) * P.ns + ws;
+                        tma_load_1d(dst + static_cast<uint32_t>(size) * EB, P.pairs + offb,
+                                    static_cast<uint32_t>(size) * EB, &full[stage]);
+                    }
                 }
                 ++it;
             }
@@ -824,50 +956,19 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             w.shi = m.shi[g];
             w.wef = m.wend[g];
 #else
-            w.shi = 0.0f;  // read below, where a clamp needs it
+            w.shi = 0.0f;  // read by visit_slot, where a clamp needs it
             w.wef = 0.0f;
 #endif
             w.err = P.err;
             const float sc = STORE == kStoreF32 ? 1.0f : m.sc[g];
-            if (r2 <= gminall) {  // interior trace: every term of the tile passes
-#pragma unroll
-                for (int p = 0; p < J / 2; ++p) {
-                    if (STORE == kStoreF32)
-                        term_pair<AMP, false, PACKED>(smem_raw, r2, base2, w, T2[p], F4[p],
-                                                      BB[p], SUM[p]);
-                    else
-                        term_pair16<AMP, false, STORE>(smem_raw, r2, base2, w, sc, T2[p],
-                                                       F4[p], BB[p], SUM[p]);
-                }
-                continue;
-            }
-            w.shi = m.shi[g];
-#pragma unroll
-            for (int gr = 0; gr < NG; ++gr) {
-                if (r2 <= gmax[gr]) {
-                    if (r2 <= gmin[gr]) {  // every lane of the group passes
-#pragma unroll
-                        for (int p = PG * gr; p < PG * (gr + 1); ++p) {
-                            if (STORE == kStoreF32)
-                                term_pair<AMP, false, PACKED>(smem_raw, r2, base2, w,
-                                                              T2[p], F4[p], BB[p], SUM[p]);
-                            else
-                                term_pair16<AMP, false, STORE>(smem_raw, r2, base2, w,
-                                                               sc, T2[p], F4[p], BB[p], SUM[p]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int p = PG * gr; p < PG * (gr + 1); ++p) {
-                            if (STORE == kStoreF32)
-                                term_pair<AMP, true, PACKED>(smem_raw, r2, base2, w,
-                                                             T2[p], F4[p], BB[p], SUM[p]);
-                            else
-                                term_pair16<AMP, true, STORE>(smem_raw, r2, base2, w,
-                                                              sc, T2[p], F4[p], BB[p], SUM[p]);
-                        }
-                    }
-                }
-            }
+            if (PAIRS && ((m.pairmask >> g) & 1u))
+                visit_slot<AMP, PACKED, GB, J, STORE, true>(
+                    smem_raw, r2, base2, static_cast<uint32_t>(m.baseb[g]), w, &m.shi[g], sc,
+                    gminall, gmax, gmin, T2, F4, BB, SUM);
+            else
+                visit_slot<AMP, PACKED, GB, J, STORE, false>(smem_raw, r2, base2, 0u, w,
+                                                             &m.shi[g], sc, gminall, gmax,
+                                                             gmin, T2, F4, BB, SUM);
         }
         if (KAHAN) {  // ACC += PART, compensated
 #pragma unroll
@@ -922,26 +1023,28 @@ __device__ __forceinline__ void ring_init(unsigned char* smem_raw, const SmemLay
 }
 
 // One tile per CTA: grid (crossline tiles, time tiles, jobs).
-template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false>
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
+          bool PAIRS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);  // ordered by the tile's first barrier
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
-                                               blockIdx.y * 32 * J, smem_raw, L, it);
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
+                                                      blockIdx.y * 32 * J, smem_raw, L, it);
 }
 
 // The same with 3 CTAs per SM (27 warps): registers are held to 72 per thread and the launcher
 // gives it stages of 32 KB, so that three CTAs fit the SM's registers and shared memory.
-template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false>
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
+          bool PAIRS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
-                                               blockIdx.y * 32 * J, smem_raw, L, it);
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
+                                                      blockIdx.y * 32 * J, smem_raw, L, it);
 }
 
 // One tile of a batched launch: problem, job of that problem, first crossline and sample.
@@ -961,7 +1064,8 @@ static_assert(sizeof(BatchParams) + 64 <= 32764, "kernel parameters are limited 
 // counter) until the list is exhausted, with the ring kept across tiles.  Problems (velocity
 // panels, sub-volumes) each have their own FwdParams.  max_inl and stage_cap are the largest
 // over the problems.  A device error (bounded wait expired) stops every CTA at its next tile.
-template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false>
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
+          bool PAIRS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2)
     fwd_batch_kernel(const __grid_constant__ BatchParams B,
                      const BatchItem* __restrict__ items, int n_items, int* next,
@@ -982,8 +1086,8 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2)
         __syncthreads();
         const BatchItem w = s_item;
         if (w.prob < 0) break;
-        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN>(B.p[w.prob], s_job, w.x0,
-                                                                  w.T0, smem_raw, L, it);
+        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
+            B.p[w.prob], s_job, w.x0, w.T0, smem_raw, L, it);
         // barrier: the tile's tables, statistics, s_item and s_job are reused next
         if (__syncthreads_or(!ok)) break;
     }
