@@ -228,7 +228,9 @@ typedef enum {
     PSM_FWD_SCALAR_G4_O3 = 10,
     PSM_FWD_PAIRS_O3 = 11, /* mirrored inlines c - d, c + d staged as pairs, 3 CTAs per SM */
     PSM_FWD_PAIRS = 12,
-    PSM_FWD_N_VARIANTS = 13
+    PSM_FWD_QUADS_O3 = 13, /* pairs, and also the crosslines x - e, x + e of each warp's x */
+    PSM_FWD_QUADS = 14,
+    PSM_FWD_N_VARIANTS = 15
 } psm_fwd_variant;
 int psm_set_variant(psm_ctx *ctx, int variant);
 int psm_get_variant(psm_ctx *ctx, int *variant);

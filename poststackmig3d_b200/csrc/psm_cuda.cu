@@ -98,26 +98,35 @@ inline bool is_j16(int variant) {
 
 inline bool is_o3(int variant) {
     return variant == PSM_FWD_PACKED_G4_O3 || variant == PSM_FWD_SCALAR_G4_O3 ||
-           variant == PSM_FWD_PAIRS_O3;
+           variant == PSM_FWD_PAIRS_O3 || variant == PSM_FWD_QUADS_O3;
+}
+
+inline bool is_pairs(int variant) {
+    return variant == PSM_FWD_PAIRS_O3 || variant == PSM_FWD_PAIRS ||
+           variant == PSM_FWD_QUADS_O3 || variant == PSM_FWD_QUADS;
 }
 
 // The variant that actually runs: 16-bit storage and compensated summation run the packed
 // skip-4 kernel, with 16 blocks a lane (16-bit storage only: compensation's partial and
-// compensation registers leave no room for 16), or built for 3 CTAs per SM, or else the
-// default build.
+// compensation registers leave no room for 16), or built for 3 CTAs per SM, each with or
+// without mirrored pairs.
 inline int effective_variant(int variant, int store, bool kahan) {
     if (variant == PSM_FWD_DEFAULT) variant = kDefaultVariant;
     if (store == psm::kStoreF32 && !kahan) return variant;
     if (!kahan && is_j16(variant)) return PSM_FWD_PACKED_G4_J16;
+    if (variant == PSM_FWD_QUADS_O3) return PSM_FWD_PAIRS_O3;  // crossline mirrors: fp32 only
+    if (variant == PSM_FWD_QUADS) return PSM_FWD_PAIRS;
+    if (is_pairs(variant)) return variant;
     return is_o3(variant) ? PSM_FWD_PACKED_G4_O3 : PSM_FWD_PACKED_G4;
 }
 
 // One instantiation of the forward kernel templates (MINB: CTAs per SM the kernel is built
 // for, 2 or 3).
 template <bool AMP_, bool PACKED_, int GB_, int J_, int STORE_, bool KAHAN_, int MINB_ = 2,
-          bool PAIRS_ = false>
+          bool PAIRS_ = false, bool CROSS_ = false>
 struct KernelTag {
-    static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_, PAIRS = PAIRS_;
+    static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_, PAIRS = PAIRS_,
+                          CROSS = CROSS_;
     static constexpr int GB = GB_, J = J_, STORE = STORE_, MINB = MINB_;
 };
 
@@ -131,9 +140,9 @@ inline int stage_cap_for(int minb, int store) {
 template <class K>
 auto grid_kernel() {
     if constexpr (K::MINB == 3)
-        return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
+        return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
     else
-        return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
+        return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
 }
 
 // Calls f(KernelTag<...>{}) for the kernel that (amp, effective variant, store, kahan) names.
@@ -142,7 +151,23 @@ cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
     using psm::kStoreBF16;
     using psm::kStoreF16;
     using psm::kStoreF32;
-    const bool j16 = is_j16(variant), o3 = is_o3(variant);
+    const bool j16 = is_j16(variant), o3 = is_o3(variant), pr = is_pairs(variant);
+    // 16-bit storage or compensated summation with mirrored pairs
+    if (pr && (store != kStoreF32 || kahan)) {
+        switch (store * 2 + (kahan ? 1 : 0)) {
+#define PSM_PAIR_CASE(ST, KA)                                                                \
+    case ST * 2 + KA:                                                                        \
+        return o3 ? f(KernelTag<AMP, true, 4, 8, ST, KA, 3, true>{})                         \
+                  : f(KernelTag<AMP, true, 4, 8, ST, KA, 2, true>{});
+            PSM_PAIR_CASE(kStoreF32, 1)
+            PSM_PAIR_CASE(kStoreBF16, 0)
+            PSM_PAIR_CASE(kStoreBF16, 1)
+            PSM_PAIR_CASE(kStoreF16, 0)
+            PSM_PAIR_CASE(kStoreF16, 1)
+#undef PSM_PAIR_CASE
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (store * 2 + (kahan ? 1 : 0)) {
         case kStoreF32 * 2:
             switch (variant) {
@@ -163,6 +188,10 @@ cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
                 case PSM_FWD_PAIRS_O3:
                     return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3, true>{});
                 case PSM_FWD_PAIRS: return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 2, true>{});
+                case PSM_FWD_QUADS_O3:
+                    return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3, true, true>{});
+                case PSM_FWD_QUADS:
+                    return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 2, true, true>{});
 
                 default: return cudaErrorInvalidValue;
             }
@@ -1267,7 +1296,7 @@ namespace {
 // kernel K; done before a stream capture, so the graph holds only the launch.
 template <class K>
 cudaError_t prepare_persistent(K, psm_batch& b) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
     const size_t smem =
         psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1285,7 +1314,7 @@ cudaError_t prepare_persistent(K, psm_batch& b) {
 
 template <class K>
 cudaError_t launch_persistent(K, const psm_batch& b, cudaStream_t s) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
     const size_t smem =
         psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
     const int w = (K::J == 16 ? 2 : 0) + b.order;

@@ -97,6 +97,7 @@ struct StageMeta {
     float sc[kMaxG];  // trace scale (16-bit storage)
     float wend[kMaxG];  // window end as float (read by the debug-bounds build)
     int baseb[kMaxG];   // paired slots: window base of the mirrored trace (see consumers)
+    float scb[kMaxG];   // paired slots, 16-bit storage: the mirrored trace's scale
     unsigned pairmask;  // bit g: slot g holds a mirrored pair of traces
     int pad2[3];
 };
@@ -505,13 +506,15 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
         ACC = add2(ACC, make_float2(v0, v1));
 }
 
-// Block pair of a mirrored pair of staged traces (inlines c - d and c + d at one crossline:
-// the same r^2, so the same travel times, sample indices, fractions and weights).  The two
+// Block pair of NT staged traces that share r^2 (mirrored inlines c - d and c + d at one
+// crossline, and for CROSS kernels also the crosslines x - e and x + e of the warp's output
+// crossline x): the same travel times, sample indices, fractions and weights.  The NT
 // interpolated values are added before the weight; each trace's window has its own base.
-template <bool AMP, bool MASK>
-__device__ __forceinline__ void term_pair2(const unsigned char* sbase, float r2, uint32_t base2a,
-                                           uint32_t base2b, const Win& w, const float2& T2,
-                                           const float2& F4, const float2& BB, float2& ACC) {
+template <bool AMP, bool MASK, int NT>
+__device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
+                                           const uint32_t (&base)[4], const Win& w,
+                                           const float2& T2, const float2& F4, const float2& BB,
+                                           float2& ACC) {
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
     const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
     float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
@@ -521,12 +524,14 @@ __device__ __forceinline__ void term_pair2(const unsigned char* sbase, float r2,
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
     const uint32_t o0 = __float_as_uint(mm.x) << 3, o1 = __float_as_uint(mm.y) << 3;
-    const float2 a0 = *reinterpret_cast<const float2*>(sbase + (base2a + o0));
-    const float2 a1 = *reinterpret_cast<const float2*>(sbase + (base2a + o1));
-    const float2 b0 = *reinterpret_cast<const float2*>(sbase + (base2b + o0));
-    const float2 b1 = *reinterpret_cast<const float2*>(sbase + (base2b + o1));
-    float2 v = add2(make_float2(fmaf(fr.x, a0.y, a0.x), fmaf(fr.y, a1.y, a1.x)),
-                    make_float2(fmaf(fr.x, b0.y, b0.x), fmaf(fr.y, b1.y, b1.x)));
+    float2 v;
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const float2 a0 = *reinterpret_cast<const float2*>(sbase + (base[n] + o0));
+        const float2 a1 = *reinterpret_cast<const float2*>(sbase + (base[n] + o1));
+        const float2 vn = make_float2(fmaf(fr.x, a0.y, a0.x), fmaf(fr.y, a1.y, a1.x));
+        v = n ? add2(v, vn) : vn;
+    }
     if (MASK) {
         v.x = r2 <= BB.x ? v.x : 0.0f;
         v.y = r2 <= BB.y ? v.y : 0.0f;
@@ -578,25 +583,65 @@ __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2
         ACC = fma2(v, make_float2(sc, sc), ACC);
 }
 
-// One block pair of a staged slot: a single trace (fp32 or 16-bit storage) or a mirrored pair.
-template <bool AMP, bool MASK, bool PACKED, int STORE, bool TWO>
-__device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2, uint32_t base2,
-                                          uint32_t base2b, const Win& w, float sc,
-                                          const float2& T2, const float2& F4, const float2& BB,
-                                          float2& ACC) {
-    if (TWO)
-        term_pair2<AMP, MASK>(sbase, r2, base2, base2b, w, T2, F4, BB, ACC);
-    else if (STORE == kStoreF32)
-        term_pair<AMP, MASK, PACKED>(sbase, r2, base2, w, T2, F4, BB, ACC);
+// Block pair of a mirrored pair of staged traces in 16-bit storage: as term_pair2, each trace's
+// interpolated value scaled by its own trace scale before the two are added.
+template <bool AMP, bool MASK, int STORE>
+__device__ __forceinline__ void term_pair2_16(const unsigned char* sbase, float r2,
+                                              uint32_t base2a, uint32_t base2b, const Win& w,
+                                              float sca, float scb, const float2& T2,
+                                              const float2& F4, const float2& BB, float2& ACC) {
+    const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
+    const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
+    float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
+    s.x = window_s<MASK>(s.x, w);                            // inside the staged windows
+    s.y = window_s<MASK>(s.y, w);
+    const float2 M = make_float2(8388608.0f, 8388608.0f);
+    const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
+    const float2 fr = sub2(s, sub2(mm, M));                  // frac
+    const uint32_t o0 = __float_as_uint(mm.x) << 2, o1 = __float_as_uint(mm.y) << 2;
+    const float2 a0 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2a + o0)));
+    const float2 a1 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2a + o1)));
+    const float2 b0 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2b + o0)));
+    const float2 b1 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2b + o1)));
+    const float2 la = make_float2(a0.x, a1.x), lb = make_float2(b0.x, b1.x);
+    const float2 va = fma2(fr, sub2(make_float2(a0.y, a1.y), la), la);  // simdInterpolate
+    const float2 vb = fma2(fr, sub2(make_float2(b0.y, b1.y), lb), lb);
+    float2 v = fma2(va, make_float2(sca, sca), mul2(vb, make_float2(scb, scb)));
+    if (MASK) {
+        v.x = r2 <= BB.x ? v.x : 0.0f;
+        v.y = r2 <= BB.y ? v.y : 0.0f;
+    }
+    if (AMP)
+        ACC = fma2(v, make_float2(q0, q1), ACC);
     else
-        term_pair16<AMP, MASK, STORE>(sbase, r2, base2, w, sc, T2, F4, BB, ACC);
+        ACC = add2(ACC, v);
+}
+
+// One block pair of a staged slot: a single trace (fp32 or 16-bit storage), or NT traces
+// sharing r^2 (mirrored inlines; 16-bit storage: NT = 2 only).
+template <bool AMP, bool MASK, bool PACKED, int STORE, int NT>
+__device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2,
+                                          const uint32_t (&base)[4], const Win& w, float sc,
+                                          float scb, const float2& T2, const float2& F4,
+                                          const float2& BB, float2& ACC) {
+    static_assert(NT == 1 || NT == 2 || (NT == 4 && STORE == kStoreF32), "traces per slot");
+    if (NT > 1 && STORE == kStoreF32)
+        term_multi<AMP, MASK, NT>(sbase, r2, base, w, T2, F4, BB, ACC);
+    else if (NT > 1)
+        term_pair2_16<AMP, MASK, STORE>(sbase, r2, base[0], base[1], w, sc, scb, T2, F4, BB,
+                                        ACC);
+    else if (STORE == kStoreF32)
+        term_pair<AMP, MASK, PACKED>(sbase, r2, base[0], w, T2, F4, BB, ACC);
+    else
+        term_pair16<AMP, MASK, STORE>(sbase, r2, base[0], w, sc, T2, F4, BB, ACC);
 }
 
 // One staged slot for one consumer warp: every block pair of the lane where some lane of its
 // group passes, without masks where every lane of the group (or of the tile) passes.
-template <bool AMP, bool PACKED, int GB, int J, int STORE, bool TWO>
-__device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2, uint32_t base2,
-                                           uint32_t base2b, Win w, const float* shi, float sc,
+template <bool AMP, bool PACKED, int GB, int J, int STORE, int NT>
+__device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
+                                           const uint32_t (&base)[4], Win w, const float* shi,
+                                           int g, int gm, float sc, float scb,
                                            float gminall, const float (&gmax)[J / GB],
                                            const float (&gmin)[J / GB], const float2 (&T2)[J / 2],
                                            const float2 (&F4)[J / 2], const float2 (&BB)[J / 2],
@@ -606,24 +651,25 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
     if (r2 <= gminall) {  // interior trace: every term of the tile passes
 #pragma unroll
         for (int p = 0; p < J / 2; ++p)
-            eval_pair<AMP, false, PACKED, STORE, TWO>(sbase, r2, base2, base2b, w, sc, T2[p],
-                                                      F4[p], BB[p], SUM[p]);
+            eval_pair<AMP, false, PACKED, STORE, NT>(sbase, r2, base, w, sc, scb,
+                                                      T2[p], F4[p], BB[p], SUM[p]);
         return;
     }
-    w.shi = *shi;
+    // clamp bound: the end of the staged window(s) (crossline mirrors: the intersection)
+    w.shi = gm >= 0 ? fminf(shi[g], shi[gm]) : shi[g];
 #pragma unroll
     for (int gr = 0; gr < NG; ++gr) {
         if (r2 <= gmax[gr]) {
             if (r2 <= gmin[gr]) {  // every lane of the group passes
 #pragma unroll
                 for (int p = PG * gr; p < PG * (gr + 1); ++p)
-                    eval_pair<AMP, false, PACKED, STORE, TWO>(sbase, r2, base2, base2b, w, sc,
-                                                              T2[p], F4[p], BB[p], SUM[p]);
+                    eval_pair<AMP, false, PACKED, STORE, NT>(sbase, r2, base, w, sc, scb,
+                                                             T2[p], F4[p], BB[p], SUM[p]);
             } else {
 #pragma unroll
                 for (int p = PG * gr; p < PG * (gr + 1); ++p)
-                    eval_pair<AMP, true, PACKED, STORE, TWO>(sbase, r2, base2, base2b, w, sc,
-                                                             T2[p], F4[p], BB[p], SUM[p]);
+                    eval_pair<AMP, true, PACKED, STORE, NT>(sbase, r2, base, w, sc,
+                                                             scb, T2[p], F4[p], BB[p], SUM[p]);
             }
         }
     }
@@ -643,14 +689,16 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
 // per CTA (ring_init); it counts the ring stages the CTA has used so far, so consecutive tiles
 // of a persistent CTA continue the ring's phases (every stage, the end-of-stream marker
 // included, is released by the consumers).  Returns false when a bounded wait expired.
-template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false>
+template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false,
+          bool CROSS = false>
 __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int x0, int T0,
                                          unsigned char* smem_raw, const SmemLayout& L,
                                          uint32_t& it) {
     static_assert(GB == 2 || GB == 4 || GB == 8, "skip groups of 2, 4 or 8 blocks");
     static_assert(J % GB == 0, "whole skip groups per lane");
     static_assert(STORE == kStoreF32 || PACKED, "16-bit storage uses packed arithmetic");
-    static_assert(!PAIRS || (STORE == kStoreF32 && PACKED), "mirrored pairs: packed fp32");
+    static_assert(!PAIRS || PACKED, "mirrored pairs use packed arithmetic");
+    static_assert(!CROSS || (PAIRS && STORE == kStoreF32), "crossline mirrors: fp32 pairs");
     constexpr int NG = J / GB;   // skip groups per lane
     constexpr int EB = store_bytes(STORE);
     // bits(2^23) << log2(EB), modulo 2^32 (see the producer)
@@ -817,7 +865,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         while (f < total && alive) {
             const int idx = f + lane;
             int ws = 0, size = 0, kc = 0, row = 0, rowb = -1, slot_size = 0;
-            float dx2 = 0.0f, shi = 0.0f, sc = 1.0f;
+            float dx2 = 0.0f, shi = 0.0f, sc = 1.0f, scb = 1.0f;
             if (idx < total) {
                 // row of flat slot idx: the last n with inl_pre[n] <= idx
                 int lo = 0, hi = n_rows - 1;
@@ -835,8 +883,10 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                 row = job.i0 + a;
                 rowb = b >= 0 ? job.i0 + b : -1;
                 trace_window<STORE>(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
-                if (STORE != kStoreF32 && size > 0)
+                if (STORE != kStoreF32 && size > 0) {
                     sc = __ldg(P.scales + static_cast<size_t>(row) * P.n_cx + kc);
+                    if (rowb >= 0) scb = __ldg(P.scales + static_cast<size_t>(rowb) * P.n_cx + kc);
+                }
                 slot_size = rowb >= 0 ? 2 * size : size;  // a pair's windows are the same
             }
             // inclusive prefix sum of slot sizes; take the lanes that fit one stage
@@ -879,6 +929,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     m.sc[slot] = sc;
                     m.wend[slot] = static_cast<float>(ws + size);
                     m.baseb[slot] = static_cast<int>(dst_rel + EB * size - EB * ws - MAGIC);
+                    m.scb[slot] = scb;
                 }
                 if (lane == 0) {
                     m.count = n;
@@ -897,7 +948,10 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     tma_load_1d(dst, src, static_cast<uint32_t>(size) * EB, &full[stage]);
                     if (rowb >= 0) {  // the mirrored trace's window right after
                         const size_t offb = (static_cast<size_t>(rowb) * P.n_cx + kc) * P.ns + ws;
-                        tma_load_1d(dst + static_cast<uint32_t>(size) * EB, P.pairs + offb,
+                        const void* srcb = STORE == kStoreF32
+                                               ? static_cast<const void*>(P.pairs + offb)
+                                               : static_cast<const void*>(P.words + offb);
+                        tma_load_1d(dst + static_cast<uint32_t>(size) * EB, srcb,
                                     static_cast<uint32_t>(size) * EB, &full[stage]);
                     }
                 }
@@ -945,30 +999,69 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
 #pragma unroll
             for (int p = 0; p < J / 2; ++p) PART[p] = make_float2(0.0f, 0.0f);
         }
+        const unsigned pmask = PAIRS ? m.pairmask : 0u;
         for (int g = 0; g < cnt; ++g) {
             const int4 md = m.m[g];
-            const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
+            const int dk = md.x - xv;
+            // CROSS: slots at crosslines xv - e and xv + e of one row share r^2 for this
+            // warp; the row's slots have consecutive crosslines, so the mirror of slot g is
+            // slot g + 2 (xv - kc).  The first of the two visits both; the second skips.
+            int gm = -1;
+            int4 mc = make_int4(0, 0, 0, 0);
+            if (CROSS && dk != 0) {
+                const int cand = g - 2 * dk;
+                if (cand >= 0 && cand < cnt) {
+                    mc = m.m[cand];
+                    if (mc.x == xv - dk && mc.y == md.y) gm = cand;
+                }
+                if (dk > 0 && gm >= 0) continue;  // visited with its mirror gm < g
+            }
+            const float r2 = trace_r2(dk, P.d_xl, __int_as_float(md.y));
             if (r2 > warpmax) continue;
-            const uint32_t base2 = static_cast<uint32_t>(md.z);
+            uint32_t base[4];
+            base[0] = static_cast<uint32_t>(md.z);
             Win w;
-            w.wsf = __int_as_float(md.w);
+            // a mirror's window can differ (its distance to the tile differs): terms that pass
+            // lie in both windows, and clamps use their intersection
+            w.wsf = gm >= 0 ? fmaxf(__int_as_float(md.w), __int_as_float(mc.w))
+                            : __int_as_float(md.w);
 #ifdef PSM_DEBUG_BOUNDS
-            w.shi = m.shi[g];
-            w.wef = m.wend[g];
+            w.shi = gm >= 0 ? fminf(m.shi[g], m.shi[gm]) : m.shi[g];
+            w.wef = gm >= 0 ? fminf(m.wend[g], m.wend[gm]) : m.wend[g];
 #else
             w.shi = 0.0f;  // read by visit_slot, where a clamp needs it
             w.wef = 0.0f;
 #endif
             w.err = P.err;
             const float sc = STORE == kStoreF32 ? 1.0f : m.sc[g];
-            if (PAIRS && ((m.pairmask >> g) & 1u))
-                visit_slot<AMP, PACKED, GB, J, STORE, true>(
-                    smem_raw, r2, base2, static_cast<uint32_t>(m.baseb[g]), w, &m.shi[g], sc,
-                    gminall, gmax, gmin, T2, F4, BB, SUM);
-            else
-                visit_slot<AMP, PACKED, GB, J, STORE, false>(smem_raw, r2, base2, 0u, w,
-                                                             &m.shi[g], sc, gminall, gmax,
-                                                             gmin, T2, F4, BB, SUM);
+            const bool two = PAIRS && ((pmask >> g) & 1u);
+            if (two) base[1] = static_cast<uint32_t>(m.baseb[g]);
+            if constexpr (CROSS) {
+              if (gm >= 0) {  // a mirror in one row has the row's pairing
+                if (two) {
+                    base[2] = static_cast<uint32_t>(mc.z);
+                    base[3] = static_cast<uint32_t>(m.baseb[gm]);
+                    visit_slot<AMP, PACKED, GB, J, STORE, 4>(smem_raw, r2, base, w, m.shi, g, gm,
+                                                             sc, 1.0f, gminall, gmax, gmin, T2,
+                                                             F4, BB, SUM);
+                } else {
+                    base[1] = static_cast<uint32_t>(mc.z);
+                    visit_slot<AMP, PACKED, GB, J, STORE, 2>(smem_raw, r2, base, w, m.shi, g, gm,
+                                                             sc, 1.0f, gminall, gmax, gmin, T2,
+                                                             F4, BB, SUM);
+                }
+                continue;
+              }
+            }
+            if (two) {
+                visit_slot<AMP, PACKED, GB, J, STORE, 2>(
+                    smem_raw, r2, base, w, m.shi, g, -1, sc,
+                    STORE == kStoreF32 ? 1.0f : m.scb[g], gminall, gmax, gmin, T2, F4, BB, SUM);
+            } else {
+                visit_slot<AMP, PACKED, GB, J, STORE, 1>(smem_raw, r2, base, w, m.shi, g, -1,
+                                                         sc, 1.0f, gminall, gmax, gmin, T2, F4,
+                                                         BB, SUM);
+            }
         }
         if (KAHAN) {  // ACC += PART, compensated
 #pragma unroll
@@ -1024,27 +1117,27 @@ __device__ __forceinline__ void ring_init(unsigned char* smem_raw, const SmemLay
 
 // One tile per CTA: grid (crossline tiles, time tiles, jobs).
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
-          bool PAIRS = false>
+          bool PAIRS = false, bool CROSS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);  // ordered by the tile's first barrier
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
-                                                      blockIdx.y * 32 * J, smem_raw, L, it);
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, CROSS>(
+        P, P.jobs[blockIdx.z], blockIdx.x * kTX, blockIdx.y * 32 * J, smem_raw, L, it);
 }
 
 // The same with 3 CTAs per SM (27 warps): registers are held to 72 per thread and the launcher
 // gives it stages of 32 KB, so that three CTAs fit the SM's registers and shared memory.
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
-          bool PAIRS = false>
+          bool PAIRS = false, bool CROSS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(P, P.jobs[blockIdx.z], blockIdx.x * kTX,
-                                                      blockIdx.y * 32 * J, smem_raw, L, it);
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, CROSS>(
+        P, P.jobs[blockIdx.z], blockIdx.x * kTX, blockIdx.y * 32 * J, smem_raw, L, it);
 }
 
 // One tile of a batched launch: problem, job of that problem, first crossline and sample.
@@ -1065,7 +1158,7 @@ static_assert(sizeof(BatchParams) + 64 <= 32764, "kernel parameters are limited 
 // panels, sub-volumes) each have their own FwdParams.  max_inl and stage_cap are the largest
 // over the problems.  A device error (bounded wait expired) stops every CTA at its next tile.
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
-          bool PAIRS = false>
+          bool PAIRS = false, bool CROSS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2)
     fwd_batch_kernel(const __grid_constant__ BatchParams B,
                      const BatchItem* __restrict__ items, int n_items, int* next,
@@ -1086,7 +1179,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2)
         __syncthreads();
         const BatchItem w = s_item;
         if (w.prob < 0) break;
-        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
+        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, CROSS>(
             B.p[w.prob], s_job, w.x0, w.T0, smem_raw, L, it);
         // barrier: the tile's tables, statistics, s_item and s_job are reused next
         if (__syncthreads_or(!ok)) break;
