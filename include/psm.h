@@ -97,7 +97,15 @@ int psm_set_vrms(psm_ctx *ctx, const float *vrms);
  * (src/migration_kernel.cpp:17-383) applied to every output inline of src/main.cpp:257-369. */
 int psm_forward(psm_ctx *ctx, float *image);
 
-/* Same, leaving the image in device memory owned by ctx (enqueued on the ctx stream). */
+/* Forward migration from host buffers in one call: traces and vrms [n_il][n_xl][n_t] (host)
+ * in, image [n_oi][n_ox][n_t] (host) out.  Pipelined: inline blocks upload on a copy stream,
+ * the output inlines whose buffers are resident migrate while later blocks upload, and image
+ * rows return on a third stream while later output inlines migrate (pinned host buffers let
+ * the copies overlap).  Leaves the traces and Vrms resident, as psm_set_traces/_vrms. */
+int psm_forward_host(psm_ctx *ctx, const float *traces, const float *vrms, float *image);
+
+/* Same as psm_forward, leaving the image in device memory owned by ctx (enqueued on the ctx
+ * stream). */
 int psm_forward_async(psm_ctx *ctx);
 int psm_synchronize(psm_ctx *ctx);
 /* Device pointer of the ctx-owned image [n_oi][n_ox][n_t] (valid until the next
@@ -228,9 +236,7 @@ typedef enum {
     PSM_FWD_SCALAR_G4_O3 = 10,
     PSM_FWD_PAIRS_O3 = 11, /* mirrored inlines c - d, c + d staged as pairs, 3 CTAs per SM */
     PSM_FWD_PAIRS = 12,
-    PSM_FWD_QUADS_O3 = 13, /* pairs, and also the crosslines x - e, x + e of each warp's x */
-    PSM_FWD_QUADS = 14,
-    PSM_FWD_N_VARIANTS = 15
+    PSM_FWD_N_VARIANTS = 13
 } psm_fwd_variant;
 int psm_set_variant(psm_ctx *ctx, int variant);
 int psm_get_variant(psm_ctx *ctx, int *variant);

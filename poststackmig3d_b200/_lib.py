@@ -61,6 +61,7 @@ _CUDA_SYMBOLS = [
     ("psm_set_vrms", ctypes.c_int, [_P, _P]),
     ("psm_forward", ctypes.c_int, [_P, _P]),
     ("psm_forward_async", ctypes.c_int, [_P]),
+    ("psm_forward_host", ctypes.c_int, [_P, _P, _P, _P]),
     ("psm_synchronize", ctypes.c_int, [_P]),
     ("psm_image_device", ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     ("psm_get_image", ctypes.c_int, [_P, _P]),

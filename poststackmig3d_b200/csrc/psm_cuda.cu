@@ -98,12 +98,11 @@ inline bool is_j16(int variant) {
 
 inline bool is_o3(int variant) {
     return variant == PSM_FWD_PACKED_G4_O3 || variant == PSM_FWD_SCALAR_G4_O3 ||
-           variant == PSM_FWD_PAIRS_O3 || variant == PSM_FWD_QUADS_O3;
+           variant == PSM_FWD_PAIRS_O3;
 }
 
 inline bool is_pairs(int variant) {
-    return variant == PSM_FWD_PAIRS_O3 || variant == PSM_FWD_PAIRS ||
-           variant == PSM_FWD_QUADS_O3 || variant == PSM_FWD_QUADS;
+    return variant == PSM_FWD_PAIRS_O3 || variant == PSM_FWD_PAIRS;
 }
 
 // The variant that actually runs: 16-bit storage and compensated summation run the packed
@@ -114,8 +113,6 @@ inline int effective_variant(int variant, int store, bool kahan) {
     if (variant == PSM_FWD_DEFAULT) variant = kDefaultVariant;
     if (store == psm::kStoreF32 && !kahan) return variant;
     if (!kahan && is_j16(variant)) return PSM_FWD_PACKED_G4_J16;
-    if (variant == PSM_FWD_QUADS_O3) return PSM_FWD_PAIRS_O3;  // crossline mirrors: fp32 only
-    if (variant == PSM_FWD_QUADS) return PSM_FWD_PAIRS;
     if (is_pairs(variant)) return variant;
     return is_o3(variant) ? PSM_FWD_PACKED_G4_O3 : PSM_FWD_PACKED_G4;
 }
@@ -123,10 +120,9 @@ inline int effective_variant(int variant, int store, bool kahan) {
 // One instantiation of the forward kernel templates (MINB: CTAs per SM the kernel is built
 // for, 2 or 3).
 template <bool AMP_, bool PACKED_, int GB_, int J_, int STORE_, bool KAHAN_, int MINB_ = 2,
-          bool PAIRS_ = false, bool CROSS_ = false>
+          bool PAIRS_ = false>
 struct KernelTag {
-    static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_, PAIRS = PAIRS_,
-                          CROSS = CROSS_;
+    static constexpr bool AMP = AMP_, PACKED = PACKED_, KAHAN = KAHAN_, PAIRS = PAIRS_;
     static constexpr int GB = GB_, J = J_, STORE = STORE_, MINB = MINB_;
 };
 
@@ -140,9 +136,9 @@ inline int stage_cap_for(int minb, int store) {
 template <class K>
 auto grid_kernel() {
     if constexpr (K::MINB == 3)
-        return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
+        return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
     else
-        return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
+        return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
 }
 
 // Calls f(KernelTag<...>{}) for the kernel that (amp, effective variant, store, kahan) names.
@@ -188,10 +184,7 @@ cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
                 case PSM_FWD_PAIRS_O3:
                     return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3, true>{});
                 case PSM_FWD_PAIRS: return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 2, true>{});
-                case PSM_FWD_QUADS_O3:
-                    return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3, true, true>{});
-                case PSM_FWD_QUADS:
-                    return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 2, true, true>{});
+
 
                 default: return cudaErrorInvalidValue;
             }
@@ -392,6 +385,9 @@ struct psm_ctx {
     int seg_rec_bytes = 0;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copied = nullptr;
+    // psm_forward_host: the device-to-host stream and the jobs in wave order
+    cudaStream_t d2h_stream = nullptr;
+    DevBuf d_jobs_waves;
 };
 
 namespace {
@@ -482,6 +478,8 @@ int psm_destroy(psm_ctx* c) {
         b->release();
     if (c->copied) cudaEventDestroy(c->copied);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->d2h_stream) cudaStreamDestroy(c->d2h_stream);
+    c->d_jobs_waves.release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSM_OK;
@@ -904,6 +902,135 @@ int psm_forward(psm_ctx* c, float* image) {
     return psm_get_image(c, image);
 }
 
+int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* image) {
+    if (!c || !traces || !vrms || !image) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    const psm_geom& g = c->g;
+    cudaStream_t s = c->stream;
+    if (!c->copy_stream)
+        PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    if (!c->d2h_stream)
+        PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking));
+    // input inlines in n_blocks consecutive blocks, uploaded in order.  Few and large: a CTA
+    // of a full-size cube runs for milliseconds, so every extra launch costs a tail of idle
+    // SMs, and an output inline's buffer spans much of the cube anyway.
+    const int n_blocks = std::min(g.n_il, 4);
+    auto block_end = [&](int b) { return static_cast<int>(int64_t(b + 1) * g.n_il / n_blocks); };
+    // a job runs in the wave of the first block after which its buffer and Vrms row are
+    // resident; the last wave is cut in two so that most of its rows stream back while the
+    // rest migrate
+    const int n_jobs = static_cast<int>(c->jobs.size());
+    std::vector<std::vector<int>> wave(n_blocks);
+    for (int k = 0; k < n_jobs; ++k) {
+        const Job& j = c->jobs[k];
+        const int need = std::max(j.i1, j.vrow + 1);
+        int b = 0;
+        while (block_end(b) < need) ++b;
+        wave[b].push_back(k);
+    }
+    std::vector<Job> order;
+    std::vector<std::pair<int, int>> chunks;  // (first job in order, count), after block b
+    std::vector<int> chunk_block;
+    for (int b = 0; b < n_blocks; ++b) {
+        const size_t w = wave[b].size();
+        const size_t chunk_jobs = b == n_blocks - 1 && w >= 16 ? (w * 3 + 3) / 4 : w;
+        for (size_t i = 0; i < w; i += chunk_jobs) {
+            const int n = static_cast<int>(std::min<size_t>(chunk_jobs, w - i));
+            chunks.emplace_back(static_cast<int>(order.size()), n);
+            chunk_block.push_back(b);
+            for (int t = 0; t < n; ++t) order.push_back(c->jobs[wave[b][i + t]]);
+        }
+    }
+    // rows each job's image fills: its own, then the rows that repeat it
+    std::vector<std::vector<int>> dup(static_cast<size_t>(g.n_oi));
+    for (const auto& cp : c->copies) dup[cp.second].push_back(cp.first);
+    PSM_CUDA_TRY(c->st, c->d_jobs_waves.ensure(std::max<size_t>(order.size(), 1) * sizeof(Job)));
+    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_jobs_waves.p, order.data(), order.size() * sizeof(Job),
+                                        cudaMemcpyHostToDevice, s));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), s));
+    std::vector<cudaEvent_t> ev(n_blocks + chunks.size(), nullptr);
+    for (auto& e : ev) {
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            for (auto& d : ev)
+                if (d) cudaEventDestroy(d);
+            return c->st.fail(PSM_ERR_CUDA, "cudaEventCreateWithFlags failed");
+        }
+    }
+    struct EventGuard {
+        std::vector<cudaEvent_t>& e;
+        ~EventGuard() {
+            for (auto& d : e) cudaEventDestroy(d);
+        }
+    } guard{ev};
+    // the copy stream starts after the ctx stream's earlier work (jobs, error word)
+    PSM_CUDA_TRY(c->st, cudaEventRecord(ev[0], s));
+    PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, ev[0], 0));
+    const size_t per_il = static_cast<size_t>(g.n_xl) * g.n_t;
+    for (int b = 0; b < n_blocks; ++b) {
+        const int lo = b ? block_end(b - 1) : 0, hi = block_end(b);
+        const size_t rows = static_cast<size_t>(hi - lo) * g.n_xl;
+        PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.as<float>() + size_t(lo) * g.n_xl * c->ns,
+                                              c->ns * sizeof(float), traces + lo * per_il,
+                                              g.n_t * sizeof(float), g.n_t * sizeof(float), rows,
+                                              cudaMemcpyHostToDevice, c->copy_stream));
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.as<float>() + lo * per_il, vrms + lo * per_il,
+                                            rows * g.n_t * sizeof(float), cudaMemcpyHostToDevice,
+                                            c->copy_stream));
+        PSM_CUDA_TRY(c->st, cudaEventRecord(ev[b], c->copy_stream));
+    }
+    const size_t row = static_cast<size_t>(g.n_ox) * g.n_t;
+    FwdParams P = volume_params(c);
+    size_t k = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        const int lo = b ? block_end(b - 1) : 0, hi = block_end(b);
+        const size_t r0 = size_t(lo) * g.n_xl, rows = size_t(hi - lo) * g.n_xl;
+        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(s, ev[b], 0));
+        if (c->store == psm::kStoreF32)
+            PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>() + r0 * c->ns,
+                                            c->pairs.as<float2>() + r0 * c->ns, rows, c->ns, s));
+        else
+            PSM_CUDA_TRY(c->st, quantize(c->data.as<float>() + r0 * c->ns,
+                                         c->words.as<uint32_t>() + r0 * c->ns,
+                                         c->scales.as<float>() + r0, rows, c->ns, c->store, s));
+        for (; k < chunks.size() && chunk_block[k] == b; ++k) {
+            FwdParams Q = P;
+            Q.jobs = c->d_jobs_waves.as<Job>() + chunks[k].first;
+            PSM_CUDA_TRY(c->st, launch_fwd(Q, chunks[k].second, g.amp_correction != 0,
+                                           c->variant, s, c->store, g.compensated != 0));
+            std::vector<int> out_rows;
+            for (int t = 0; t < chunks[k].second; ++t) {
+                const int r = order[chunks[k].first + t].row;
+                out_rows.push_back(r);
+                for (int d : dup[r]) {  // padded output inlines repeat the edge inline
+                    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.as<float>() + d * row,
+                                                        c->image.as<float>() + r * row,
+                                                        row * sizeof(float),
+                                                        cudaMemcpyDeviceToDevice, s));
+                    out_rows.push_back(d);
+                }
+            }
+            cudaEvent_t done = ev[n_blocks + k];
+            PSM_CUDA_TRY(c->st, cudaEventRecord(done, s));
+            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, done, 0));
+            std::sort(out_rows.begin(), out_rows.end());
+            for (size_t i = 0; i < out_rows.size();) {  // runs of consecutive rows
+                size_t e = i + 1;
+                while (e < out_rows.size() && out_rows[e] == out_rows[e - 1] + 1) ++e;
+                PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + out_rows[i] * row,
+                                                    c->image.as<float>() + out_rows[i] * row,
+                                                    (e - i) * row * sizeof(float),
+                                                    cudaMemcpyDeviceToHost, c->d2h_stream));
+                i = e;
+            }
+        }
+    }
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
+    c->have_traces = c->have_vrms = true;
+    return read_device_error(c);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------- adjoint, LSM
@@ -1296,7 +1423,7 @@ namespace {
 // kernel K; done before a stream capture, so the graph holds only the launch.
 template <class K>
 cudaError_t prepare_persistent(K, psm_batch& b) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
     const size_t smem =
         psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1314,7 +1441,7 @@ cudaError_t prepare_persistent(K, psm_batch& b) {
 
 template <class K>
 cudaError_t launch_persistent(K, const psm_batch& b, cudaStream_t s) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS, K::CROSS>;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
     const size_t smem =
         psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
     const int w = (K::J == 16 ? 2 : 0) + b.order;

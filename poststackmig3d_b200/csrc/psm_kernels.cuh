@@ -506,13 +506,12 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
         ACC = add2(ACC, make_float2(v0, v1));
 }
 
-// Block pair of NT staged traces that share r^2 (mirrored inlines c - d and c + d at one
-// crossline, and for CROSS kernels also the crosslines x - e and x + e of the warp's output
-// crossline x): the same travel times, sample indices, fractions and weights.  The NT
+// Block pair of NT staged traces that share r^2 (the mirrored inlines c - d and c + d at one
+// crossline): the same travel times, sample indices, fractions and weights.  The NT
 // interpolated values are added before the weight; each trace's window has its own base.
 template <bool AMP, bool MASK, int NT>
 __device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
-                                           const uint32_t (&base)[4], const Win& w,
+                                           const uint32_t (&base)[2], const Win& w,
                                            const float2& T2, const float2& F4, const float2& BB,
                                            float2& ACC) {
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
@@ -621,10 +620,10 @@ __device__ __forceinline__ void term_pair2_16(const unsigned char* sbase, float 
 // sharing r^2 (mirrored inlines; 16-bit storage: NT = 2 only).
 template <bool AMP, bool MASK, bool PACKED, int STORE, int NT>
 __device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2,
-                                          const uint32_t (&base)[4], const Win& w, float sc,
+                                          const uint32_t (&base)[2], const Win& w, float sc,
                                           float scb, const float2& T2, const float2& F4,
                                           const float2& BB, float2& ACC) {
-    static_assert(NT == 1 || NT == 2 || (NT == 4 && STORE == kStoreF32), "traces per slot");
+    static_assert(NT == 1 || NT == 2, "traces per slot");
     if (NT > 1 && STORE == kStoreF32)
         term_multi<AMP, MASK, NT>(sbase, r2, base, w, T2, F4, BB, ACC);
     else if (NT > 1)
@@ -640,8 +639,8 @@ __device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2,
 // group passes, without masks where every lane of the group (or of the tile) passes.
 template <bool AMP, bool PACKED, int GB, int J, int STORE, int NT>
 __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
-                                           const uint32_t (&base)[4], Win w, const float* shi,
-                                           int g, int gm, float sc, float scb,
+                                           const uint32_t (&base)[2], Win w, const float* shi,
+                                           float sc, float scb,
                                            float gminall, const float (&gmax)[J / GB],
                                            const float (&gmin)[J / GB], const float2 (&T2)[J / 2],
                                            const float2 (&F4)[J / 2], const float2 (&BB)[J / 2],
@@ -655,8 +654,7 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
                                                       T2[p], F4[p], BB[p], SUM[p]);
         return;
     }
-    // clamp bound: the end of the staged window(s) (crossline mirrors: the intersection)
-    w.shi = gm >= 0 ? fminf(shi[g], shi[gm]) : shi[g];
+    w.shi = *shi;
 #pragma unroll
     for (int gr = 0; gr < NG; ++gr) {
         if (r2 <= gmax[gr]) {
@@ -689,8 +687,7 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
 // per CTA (ring_init); it counts the ring stages the CTA has used so far, so consecutive tiles
 // of a persistent CTA continue the ring's phases (every stage, the end-of-stream marker
 // included, is released by the consumers).  Returns false when a bounded wait expired.
-template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false,
-          bool CROSS = false>
+template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false>
 __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int x0, int T0,
                                          unsigned char* smem_raw, const SmemLayout& L,
                                          uint32_t& it) {
@@ -698,7 +695,6 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
     static_assert(J % GB == 0, "whole skip groups per lane");
     static_assert(STORE == kStoreF32 || PACKED, "16-bit storage uses packed arithmetic");
     static_assert(!PAIRS || PACKED, "mirrored pairs use packed arithmetic");
-    static_assert(!CROSS || (PAIRS && STORE == kStoreF32), "crossline mirrors: fp32 pairs");
     constexpr int NG = J / GB;   // skip groups per lane
     constexpr int EB = store_bytes(STORE);
     // bits(2^23) << log2(EB), modulo 2^32 (see the producer)
@@ -1002,65 +998,31 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         const unsigned pmask = PAIRS ? m.pairmask : 0u;
         for (int g = 0; g < cnt; ++g) {
             const int4 md = m.m[g];
-            const int dk = md.x - xv;
-            // CROSS: slots at crosslines xv - e and xv + e of one row share r^2 for this
-            // warp; the row's slots have consecutive crosslines, so the mirror of slot g is
-            // slot g + 2 (xv - kc).  The first of the two visits both; the second skips.
-            int gm = -1;
-            int4 mc = make_int4(0, 0, 0, 0);
-            if (CROSS && dk != 0) {
-                const int cand = g - 2 * dk;
-                if (cand >= 0 && cand < cnt) {
-                    mc = m.m[cand];
-                    if (mc.x == xv - dk && mc.y == md.y) gm = cand;
-                }
-                if (dk > 0 && gm >= 0) continue;  // visited with its mirror gm < g
-            }
-            const float r2 = trace_r2(dk, P.d_xl, __int_as_float(md.y));
+            const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
             if (r2 > warpmax) continue;
-            uint32_t base[4];
+            uint32_t base[2];
             base[0] = static_cast<uint32_t>(md.z);
             Win w;
-            // a mirror's window can differ (its distance to the tile differs): terms that pass
-            // lie in both windows, and clamps use their intersection
-            w.wsf = gm >= 0 ? fmaxf(__int_as_float(md.w), __int_as_float(mc.w))
-                            : __int_as_float(md.w);
+            w.wsf = __int_as_float(md.w);
 #ifdef PSM_DEBUG_BOUNDS
-            w.shi = gm >= 0 ? fminf(m.shi[g], m.shi[gm]) : m.shi[g];
-            w.wef = gm >= 0 ? fminf(m.wend[g], m.wend[gm]) : m.wend[g];
+            w.shi = m.shi[g];
+            w.wef = m.wend[g];
 #else
             w.shi = 0.0f;  // read by visit_slot, where a clamp needs it
             w.wef = 0.0f;
 #endif
             w.err = P.err;
             const float sc = STORE == kStoreF32 ? 1.0f : m.sc[g];
-            const bool two = PAIRS && ((pmask >> g) & 1u);
-            if (two) base[1] = static_cast<uint32_t>(m.baseb[g]);
-            if constexpr (CROSS) {
-              if (gm >= 0) {  // a mirror in one row has the row's pairing
-                if (two) {
-                    base[2] = static_cast<uint32_t>(mc.z);
-                    base[3] = static_cast<uint32_t>(m.baseb[gm]);
-                    visit_slot<AMP, PACKED, GB, J, STORE, 4>(smem_raw, r2, base, w, m.shi, g, gm,
-                                                             sc, 1.0f, gminall, gmax, gmin, T2,
-                                                             F4, BB, SUM);
-                } else {
-                    base[1] = static_cast<uint32_t>(mc.z);
-                    visit_slot<AMP, PACKED, GB, J, STORE, 2>(smem_raw, r2, base, w, m.shi, g, gm,
-                                                             sc, 1.0f, gminall, gmax, gmin, T2,
-                                                             F4, BB, SUM);
-                }
-                continue;
-              }
-            }
-            if (two) {
+            if (PAIRS && ((pmask >> g) & 1u)) {
+                base[1] = static_cast<uint32_t>(m.baseb[g]);
                 visit_slot<AMP, PACKED, GB, J, STORE, 2>(
-                    smem_raw, r2, base, w, m.shi, g, -1, sc,
-                    STORE == kStoreF32 ? 1.0f : m.scb[g], gminall, gmax, gmin, T2, F4, BB, SUM);
+                    smem_raw, r2, base, w, &m.shi[g], sc, STORE == kStoreF32 ? 1.0f : m.scb[g],
+                    gminall, gmax, gmin, T2, F4, BB, SUM);
             } else {
-                visit_slot<AMP, PACKED, GB, J, STORE, 1>(smem_raw, r2, base, w, m.shi, g, -1,
-                                                         sc, 1.0f, gminall, gmax, gmin, T2, F4,
-                                                         BB, SUM);
+                base[1] = 0u;
+                visit_slot<AMP, PACKED, GB, J, STORE, 1>(smem_raw, r2, base, w, &m.shi[g], sc,
+                                                         1.0f, gminall, gmax, gmin, T2, F4, BB,
+                                                         SUM);
             }
         }
         if (KAHAN) {  // ACC += PART, compensated
@@ -1117,26 +1079,26 @@ __device__ __forceinline__ void ring_init(unsigned char* smem_raw, const SmemLay
 
 // One tile per CTA: grid (crossline tiles, time tiles, jobs).
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
-          bool PAIRS = false, bool CROSS = false>
+          bool PAIRS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);  // ordered by the tile's first barrier
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, CROSS>(
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
         P, P.jobs[blockIdx.z], blockIdx.x * kTX, blockIdx.y * 32 * J, smem_raw, L, it);
 }
 
 // The same with 3 CTAs per SM (27 warps): registers are held to 72 per thread and the launcher
 // gives it stages of 32 KB, so that three CTAs fit the SM's registers and shared memory.
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
-          bool PAIRS = false, bool CROSS = false>
+          bool PAIRS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, CROSS>(
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
         P, P.jobs[blockIdx.z], blockIdx.x * kTX, blockIdx.y * 32 * J, smem_raw, L, it);
 }
 
@@ -1158,7 +1120,7 @@ static_assert(sizeof(BatchParams) + 64 <= 32764, "kernel parameters are limited 
 // panels, sub-volumes) each have their own FwdParams.  max_inl and stage_cap are the largest
 // over the problems.  A device error (bounded wait expired) stops every CTA at its next tile.
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
-          bool PAIRS = false, bool CROSS = false>
+          bool PAIRS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2)
     fwd_batch_kernel(const __grid_constant__ BatchParams B,
                      const BatchItem* __restrict__ items, int n_items, int* next,
@@ -1179,7 +1141,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2)
         __syncthreads();
         const BatchItem w = s_item;
         if (w.prob < 0) break;
-        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, CROSS>(
+        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
             B.p[w.prob], s_job, w.x0, w.T0, smem_raw, L, it);
         // barrier: the tile's tables, statistics, s_item and s_job are reused next
         if (__syncthreads_or(!ok)) break;

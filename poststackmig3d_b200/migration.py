@@ -354,6 +354,20 @@ class Migrator:
         check(self._L.psm_forward(self._ctx, _addr(out)), self._err)
         return out
 
+    def forward_host(self, traces, vrms, out=None):
+        """Upload, migrate and download in one pipelined call (psm_forward_host): traces and
+        vrms are host float32 [n_il][n_xl][n_t] (numpy or pinned CPU tensors)."""
+        g = self.geom
+        if out is None:
+            out = np.empty(self.image_shape(), dtype=np.float32)
+        if isinstance(traces, np.ndarray):
+            traces = _f32(traces, (g.n_il, g.n_xl, g.n_t))
+        if isinstance(vrms, np.ndarray):
+            vrms = _f32(vrms, (g.n_il, g.n_xl, g.n_t))
+        check(self._L.psm_forward_host(self._ctx, _addr(traces), _addr(vrms), _addr(out)),
+              self._err)
+        return out
+
     def forward_async(self) -> None:
         check(self._L.psm_forward_async(self._ctx), self._err)
 
@@ -407,8 +421,7 @@ class Migrator:
 
     VARIANTS = {1: "scalar/g2", 2: "scalar/g4", 3: "packed/g2", 4: "packed/g4",
                 5: "packed/g4/j16", 6: "scalar/g4/j16", 7: "packed/g8", 8: "scalar/g8",
-                9: "packed/g4/o3", 10: "scalar/g4/o3", 11: "pairs/o3", 12: "pairs",
-                13: "quads/o3", 14: "quads"}
+                9: "packed/g4/o3", 10: "scalar/g4/o3", 11: "pairs/o3", 12: "pairs"}
 
     def set_variant(self, variant: int) -> None:
         check(self._L.psm_set_variant(self._ctx, int(variant)), self._err)
