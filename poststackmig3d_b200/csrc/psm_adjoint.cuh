@@ -139,8 +139,10 @@ __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
     __syncwarp();
 }
 
-template <bool AMP>
-__global__ void __launch_bounds__(32 * (kTX + 1), 2) adj_kernel(const AdjParams A) {
+// MINB: CTAs per SM the kernel is built for (the host gives 3-CTA launches 32 KB stages): the
+// kernel is bound by the latency of its shared-memory atomics, which more warps hide.
+template <bool AMP, int MINB = 2>
+__global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjParams A) {
     const FwdParams& P = A.F;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const AdjLayout L = adj_layout(P.max_inl, P.stage_cap);

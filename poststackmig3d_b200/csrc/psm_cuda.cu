@@ -1038,7 +1038,21 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
 namespace {
 
 constexpr int kAdjStageCapMin = 12288;  // fp32 samples per adjoint ring stage (48 KB)
-inline int adj_stage_cap(int ns) { return std::max(kAdjStageCapMin, ns); }
+constexpr int kAdjStageCapO3 = 8192;    // the same for 3 CTAs per SM (32 KB)
+inline int adj_stage_cap(int ns, int minb = 2) {
+    return std::max(minb == 3 ? kAdjStageCapO3 : kAdjStageCapMin, ns);
+}
+
+template <bool AMP, int MINB>
+cudaError_t launch_adj(const psm::AdjParams& A, dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(psm::adj_kernel<AMP, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    psm::adj_kernel<AMP, MINB><<<grid, block, smem, s>>>(A);
+    return cudaGetLastError();
+}
 
 inline unsigned grid_for(size_t n) {
     return static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 8)));
@@ -1061,27 +1075,26 @@ int adjoint_dev(psm_ctx* c, const float* d_rows, float* d_out) {
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(d_out, 0, n_tr * c->ns * sizeof(float), c->stream));
     psm::AdjParams A{};
     A.F = volume_params(c);
-    A.F.stage_cap = adj_stage_cap(c->ns);
     A.image = job_img;
     A.data = d_out;
-    const size_t smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap).total;
+    // 3 CTAs per SM when their 32 KB stages (and the inline tables) fit a third of the SM
+    A.F.stage_cap = adj_stage_cap(c->ns, 3);
+    size_t smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap).total;
+    const bool o3 = smem <= 75 * 1024;
+    if (!o3) {
+        A.F.stage_cap = adj_stage_cap(c->ns);
+        smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap).total;
+    }
     if (smem > kMaxDynSmem)
         return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t / aperture too large for the adjoint ring");
     dim3 grid((c->g.n_ox + psm::kTX - 1) / psm::kTX, (c->g.n_t + psm::kTT - 1) / psm::kTT,
               n_jobs);
     dim3 block(32 * (psm::kTX + 1));
-    if (c->g.amp_correction) {
-        PSM_CUDA_TRY(c->st, cudaFuncSetAttribute(psm::adj_kernel<true>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 static_cast<int>(smem)));
-        psm::adj_kernel<true><<<grid, block, smem, c->stream>>>(A);
-    } else {
-        PSM_CUDA_TRY(c->st, cudaFuncSetAttribute(psm::adj_kernel<false>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 static_cast<int>(smem)));
-        psm::adj_kernel<false><<<grid, block, smem, c->stream>>>(A);
-    }
-    PSM_CUDA_TRY(c->st, cudaGetLastError());
+    const bool amp = c->g.amp_correction != 0;
+    PSM_CUDA_TRY(c->st, o3 ? (amp ? launch_adj<true, 3>(A, grid, block, smem, c->stream)
+                                  : launch_adj<false, 3>(A, grid, block, smem, c->stream))
+                           : (amp ? launch_adj<true, 2>(A, grid, block, smem, c->stream)
+                                  : launch_adj<false, 2>(A, grid, block, smem, c->stream)));
     return PSM_OK;
 }
 
