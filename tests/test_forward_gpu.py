@@ -181,14 +181,19 @@ def test_golden_constant_velocity_cases():
         assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (name, rms, mx)
 
 
-@pytest.mark.parametrize("seed,pad_il,pad_xl,n_il", [(41, 3, 2, 30), (42, 0, 0, 7), (43, 5, 1, 3)])
-def test_forward_host_pipeline_equals_resident_forward(seed, pad_il, pad_xl, n_il):
+@pytest.mark.parametrize("seed,pad_il,pad_xl,n_il,precision,compensated",
+                         [(41, 3, 2, 30, "f32", False), (42, 0, 0, 7, "f32", False),
+                          (43, 5, 1, 3, "f32", False), (44, 2, 1, 20, "bf16", False),
+                          (45, 1, 0, 18, "f32", True)])
+def test_forward_host_pipeline_equals_resident_forward(seed, pad_il, pad_xl, n_il, precision,
+                                                       compensated):
     """psm_forward_host (inline blocks uploaded on a copy stream, waves of output inlines,
     rows streamed back) gives the resident forward's image bit for bit, repeated padded rows
-    included, twice in a row."""
+    included, twice in a row; with 16-bit storage and with compensated summation too."""
+    import dataclasses
     W = S.random_workload(seed, n_il, 11, 230, vel_kind="lateral", pad_il=pad_il,
                           pad_xl=pad_xl, d_il=60.0)
-    g = geometry_for(W)
+    g = dataclasses.replace(geometry_for(W), precision=precision, compensated=compensated)
     ref, _, _ = gpu_forward(W, g)
     with Migrator(0) as m:
         m.set_geometry(g)
