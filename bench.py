@@ -435,10 +435,16 @@ def run_lsm(args):
     lhs = float(np.sum(m.forward().astype(np.float64) * m1))
     rhs = float(np.sum(d1.astype(np.float64) * m.adjoint(m1)))
     iters = 10
+    props = torch.cuda.get_device_properties(0)
+    uuid = str(getattr(props, "uuid", ""))
+    clk = ClockSampler(("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or "0"))
     torch.cuda.synchronize()
+    clk.start()
+    time.sleep(0.25)
     t = time.perf_counter()
     img, hist = m.lsm_cg(d, iters)
     secs = time.perf_counter() - t
+    clk.stop()
     m.close()
     line = {"metric": "least-squares migration, 10 CG iterations", "value": secs / iters * 1e3,
             "unit": "ms/iteration", "higher_is_better": False,
@@ -448,7 +454,8 @@ def run_lsm(args):
             "relative_residual": float(hist[-1] / hist[0]),
             "residual_history": [float(h / hist[0]) for h in hist],
             "dot_product_rel_err": abs(lhs - rhs) / max(abs(lhs), abs(rhs)),
-            "dtype": "f32 operators, f64 CG scalars", "data": "synthetic (seeded)"}
+            "dtype": "f32 operators, f64 CG scalars", "data": "synthetic (seeded)",
+            "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -507,8 +507,9 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
 }
 
 // Block pair of NT staged traces that share r^2 (the mirrored inlines c - d and c + d at one
-// crossline): the same travel times, sample indices, fractions and weights.  The NT
-// interpolated values are added before the weight; each trace's window has its own base.
+// crossline): the same travel times, sample indices, fractions and weights.  Interpolation is
+// linear in the samples, so the NT staged (d[lo], d[lo+1] - d[lo]) pairs are added first and
+// interpolated once; each trace's window has its own base.
 template <bool AMP, bool MASK, int NT>
 __device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
                                            const uint32_t (&base)[2], const Win& w,
@@ -523,14 +524,14 @@ __device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
     const uint32_t o0 = __float_as_uint(mm.x) << 3, o1 = __float_as_uint(mm.y) << 3;
-    float2 v;
+    float2 a0 = *reinterpret_cast<const float2*>(sbase + (base[0] + o0));
+    float2 a1 = *reinterpret_cast<const float2*>(sbase + (base[0] + o1));
 #pragma unroll
-    for (int n = 0; n < NT; ++n) {
-        const float2 a0 = *reinterpret_cast<const float2*>(sbase + (base[n] + o0));
-        const float2 a1 = *reinterpret_cast<const float2*>(sbase + (base[n] + o1));
-        const float2 vn = make_float2(fmaf(fr.x, a0.y, a0.x), fmaf(fr.y, a1.y, a1.x));
-        v = n ? add2(v, vn) : vn;
+    for (int n = 1; n < NT; ++n) {
+        a0 = add2(a0, *reinterpret_cast<const float2*>(sbase + (base[n] + o0)));
+        a1 = add2(a1, *reinterpret_cast<const float2*>(sbase + (base[n] + o1)));
     }
+    float2 v = make_float2(fmaf(fr.x, a0.y, a0.x), fmaf(fr.y, a1.y, a1.x));
     if (MASK) {
         v.x = r2 <= BB.x ? v.x : 0.0f;
         v.y = r2 <= BB.y ? v.y : 0.0f;
