@@ -5,6 +5,12 @@ independent, so there is no collective on the data path; the image rows are gath
 rank 0 at the end.  The reference has no counterpart (one process, OpenMP over output inlines,
 src/main.cpp:291-361).
 
+Least-squares migration sharded the same way (lsm_sharded): image vectors are split in the
+output-inline slabs, data vectors are held on each rank's halo of input inlines.  The adjoint
+(spray) of a slab reaches its whole halo, and neighbouring halos overlap, so its contributions
+are summed over the ranks that share an inline (halo_sum, point-to-point), and the CG inner
+products are summed over ranks (each data inline counted once, by its owner).
+
 The split balances work: the weight of an output inline is its term count when known
 (Migrator.count_terms_rows), else 1.
 """
@@ -85,3 +91,171 @@ def migrate_sharded(g: Geometry, traces: np.ndarray, vrms: np.ndarray, rank: int
     slab, rows = migrate_shard(g, traces, vrms, rank, world, device, weight, migrate)
     return gather_rows(g, slab, rows, rank, world, weight,
                        device=f"cuda:{device}" if nccl else None)
+
+
+# ----------------------------------------------------------------------------- sharded LSM
+
+
+def owned_ranges(slabs):
+    """Input inlines [a, b) each rank owns for the data-space inner products: consecutive
+    ranges that partition the cube's inlines, each inside its rank's halo [i0, i1) (halos of
+    neighbouring slabs overlap or touch, since every output inline reads its own centre)."""
+    out, e = [], 0
+    for o0, o1, i0, i1 in slabs:
+        if o1 <= o0:
+            out.append((e, e))
+            continue
+        if i0 > e:
+            raise ValueError(f"halo [{i0}, {i1}) leaves inlines [{e}, {i0}) to no rank")
+        out.append((e, max(e, i1)))
+        e = max(e, i1)
+    return out
+
+
+class _Comm:
+    """Exchanges of numpy arrays between ranks: CPU tensors (gloo) or device tensors (NCCL,
+    `device` set)."""
+
+    def __init__(self, rank: int, world: int, device=None):
+        self.rank, self.world, self.device = rank, world, device
+
+    def _t(self, a):
+        import torch
+        t = torch.from_numpy(np.ascontiguousarray(a))
+        return t.to(self.device) if self.device is not None else t
+
+    def allsum(self, x: float) -> float:
+        """Sum of one float64 per rank, added in rank order (the same bits on every rank)."""
+        if self.world == 1:
+            return float(x)
+        import torch
+        import torch.distributed as dist
+        mine = self._t(np.array([x], dtype=np.float64))
+        parts = [torch.empty_like(mine) for _ in range(self.world)]
+        dist.all_gather(parts, mine)
+        total = 0.0
+        for t in parts:
+            total += float(t.cpu().numpy()[0])
+        return total
+
+    def halo_sum(self, part: np.ndarray, halo) -> np.ndarray:
+        """This rank's halo of the sum over ranks of their halo arrays: every pair of ranks
+        whose halos overlap swaps the overlap; the terms are added in rank order, so every
+        rank holding an inline gets the same bits."""
+        if self.world == 1:
+            return part
+        import torch
+        import torch.distributed as dist
+        i0, i1 = halo[self.rank]
+        works, recv = [], {}
+        for s in range(self.world):
+            if s == self.rank:
+                continue
+            a0, a1 = max(i0, halo[s][0]), min(i1, halo[s][1])
+            if a1 <= a0:
+                continue
+            send = self._t(part[a0 - i0:a1 - i0])
+            buf = torch.empty_like(send)
+            works.append(dist.isend(send, dst=s))
+            works.append(dist.irecv(buf, src=s))
+            recv[s] = (a0, a1, buf)
+        for w in works:
+            w.wait()
+        total = np.zeros_like(part)
+        for s in range(self.world):
+            if s == self.rank:
+                total += part
+            elif s in recv:
+                a0, a1, buf = recv[s]
+                total[a0 - i0:a1 - i0] += buf.cpu().numpy()
+        return total
+
+
+class _SlabOps:
+    """Forward (migration) and adjoint (spray) of one slab on a GPU, host arrays in and out."""
+
+    def __init__(self, lg: Geometry, vrms: np.ndarray, device: int):
+        self.m = Migrator(device)
+        self.m.set_geometry(lg)
+        self.m.set_vrms(vrms)
+
+    def forward(self, d: np.ndarray) -> np.ndarray:
+        self.m.set_traces(d)
+        return self.m.forward()
+
+    def adjoint(self, rows: np.ndarray) -> np.ndarray:
+        return self.m.adjoint(rows)
+
+    def close(self):
+        self.m.close()
+
+
+def lsm_sharded(g: Geometry, data: np.ndarray, vrms: np.ndarray, rank: int, world: int,
+                iters: int, device: int = 0, weight=None, make_ops: Optional[Callable] = None,
+                nccl: bool = False):
+    """CGLS on min ||M^T m - data||^2 (M the migration, M^T the spray), as Migrator.lsm_cg, with
+    the image split in output-inline slabs over `world` ranks.  Returns (slab, this rank's image
+    rows [o1 - o0][n_ox][n_t], data-residual norms [iters + 1]); gather_rows collects the
+    image.  data and vrms are the whole cube's [n_il][n_xl][n_t] (only this rank's halo is
+    read).  `make_ops` (local geometry, halo Vrms, device) -> object with forward(halo data)
+    -> rows and adjoint(rows) -> halo data replaces the GPU operators (tests).
+
+    Per iteration: one adjoint and one forward per rank on its slab, one halo exchange (the
+    adjoint's contributions to inlines that neighbouring halos share) and three scalar sums.
+    Every rank takes the same collective steps, empty slabs included."""
+    slabs = split_slabs(g, world, weight)
+    owned = owned_ranges(slabs)
+    halo = [(s[2], s[3]) if s[1] > s[0] else (a, a) for s, (a, _) in zip(slabs, owned)]
+    o0, o1 = slabs[rank][0], slabs[rank][1]
+    i0, i1 = halo[rank]
+    a0, a1 = owned[rank]
+    comm = _Comm(rank, world, f"cuda:{device}" if nccl else None)
+    shape_d = (i1 - i0, g.n_xl, g.n_t)
+    shape_m = (max(o1 - o0, 0), g.n_ox, g.n_t)
+    ops = None
+    if o1 > o0:
+        lg = slab_geometry(g, slabs[rank])
+        ops = (make_ops or _SlabOps)(lg, np.ascontiguousarray(vrms[i0:i1], dtype=np.float32),
+                                     device)
+
+    def fwd(d):
+        return np.asarray(ops.forward(d), dtype=np.float32) if ops else np.zeros(shape_m,
+                                                                                  np.float32)
+
+    def adj(rows):
+        part = (np.asarray(ops.adjoint(rows), dtype=np.float32) if ops
+                else np.zeros(shape_d, np.float32))
+        return comm.halo_sum(part, halo)
+
+    def ddot(x, y):  # data space: owned inlines only
+        lo, hi = a0 - i0, a1 - i0
+        return comm.allsum(float(np.dot(x[lo:hi].ravel().astype(np.float64),
+                                        y[lo:hi].ravel().astype(np.float64))))
+
+    def mdot(x, y):
+        return comm.allsum(float(np.dot(x.ravel().astype(np.float64),
+                                        y.ravel().astype(np.float64))))
+
+    try:
+        r = np.ascontiguousarray(data[i0:i1], dtype=np.float32).copy()  # d - M^T 0
+        m = np.zeros(shape_m, dtype=np.float32)
+        hist = [ddot(r, r)]
+        s = fwd(r)
+        p = s.copy()
+        gamma = mdot(s, s)
+        for _ in range(iters):
+            q = adj(p)                                     # q = M^T p
+            delta = ddot(q, q)
+            alpha = np.float32(gamma / delta if delta > 0.0 else 0.0)
+            m += alpha * p
+            r -= alpha * q
+            hist.append(ddot(r, r))
+            s = fwd(r)                                     # s = M r
+            gamma_new = mdot(s, s)
+            beta = np.float32(gamma_new / gamma if gamma > 0.0 else 0.0)
+            gamma = gamma_new
+            p = s + beta * p
+    finally:
+        if ops is not None and hasattr(ops, "close"):
+            ops.close()
+    return slabs[rank], m, np.sqrt(np.maximum(np.array(hist), 0.0))
