@@ -12,7 +12,10 @@
 // zeroed shared-memory accumulator holding one fp32 window per listed trace; consumers add
 // into it with shared-memory atomics; once a stage is released, the producer adds every
 // window into the data cube in HBM with a TMA bulk reduction (cp.reduce.async.bulk .add.f32)
-// and waits for the reduction to have read the stage before zeroing and reusing it.
+// and waits for the reduction to have read the stage before zeroing and reusing it.  As in
+// the forward, the traces at inlines c - d and c + d of one crossline (mirrored about the
+// output inline c) have the same r^2 to every output point: they share one slot with two
+// windows, and each term's travel time, fraction and weight are computed once for both.
 #pragma once
 
 #include "psm_kernels.cuh"
@@ -26,11 +29,14 @@ struct AdjParams {
 };
 
 struct AdjMeta {
-    int count;         // windows in this stage, -1 = end of stream
-    int pad[3];
+    int count;         // slots in this stage, -1 = end of stream
+    unsigned pairmask; // bit k: slot k holds a mirrored pair (a second window after the first)
+    int pad[2];
     int4 m[kMaxG];     // crossline, dx^2 (bits), window base (smem bytes), window start (f32)
     float shi[kMaxG];  // largest s whose lo and lo + 1 stay inside the window
     int4 g[kMaxG];     // flush: cube row, crossline, window start, window length (samples)
+    int baseb[kMaxG];  // paired slots: window base of the mirrored trace
+    int rowb[kMaxG];   // paired slots: cube row of the mirrored trace (-1: none)
 };
 
 struct AdjLayout {
@@ -103,11 +109,12 @@ __device__ __forceinline__ void adj_window(const FwdParams& P, const TileStats& 
     *shi_out = fminf(P.ntm1m, __uint_as_float(__float_as_uint(static_cast<float>(we - 1)) - 1u));
 }
 
-// One term of the transpose (scalar FP32): the forward's s, frac and q, then two atomic adds.
-template <bool AMP, bool MASK>
-__device__ __forceinline__ void adj_term(unsigned char* sbase, float r2, uint32_t base2,
-                                         float wsf, float shi, float T2, float F4, float BB,
-                                         float MK) {
+// One term of the transpose (scalar FP32) for the NT traces of a slot (a mirrored pair: the
+// same r^2): the forward's s, frac and q, then two atomic adds into each trace's window.
+template <bool AMP, bool MASK, int NT>
+__device__ __forceinline__ void adj_term(unsigned char* sbase, float r2,
+                                         const uint32_t (&base)[2], float wsf, float shi,
+                                         float T2, float F4, float BB, float MK) {
     const float t2 = __fmaf_rn(F4, r2, T2);
     const float q = rsqrtf(t2);
     const float s = fminf(fmaxf(t2 * q, wsf), shi);
@@ -117,13 +124,44 @@ __device__ __forceinline__ void adj_term(unsigned char* sbase, float r2, uint32_
     const float c = AMP ? MK * q : MK;
     const float c1 = c * fr;
     const float c0 = c - c1;
-    float* p = reinterpret_cast<float*>(sbase + (base2 + (__float_as_uint(mm) << 2)));
-    atomicAdd(p, c0);
-    atomicAdd(p + 1, c1);
+    const uint32_t o = __float_as_uint(mm) << 2;
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        float* p = reinterpret_cast<float*>(sbase + (base[n] + o));
+        atomicAdd(p, c0);
+        atomicAdd(p + 1, c1);
+    }
+}
+
+// One slot for one consumer warp: the groups of blocks where some lane passes, without masks
+// where every lane of the group passes.
+template <bool AMP, int NT>
+__device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2,
+                                          const uint32_t (&base)[2], float wsf, float shi,
+                                          const float (&gmax)[2], const float (&gmin)[2],
+                                          const float (&T2)[kJ], const float (&F4)[kJ],
+                                          const float (&BB)[kJ], const float (&MK)[kJ]) {
+#pragma unroll
+    for (int gr = 0; gr < 2; ++gr) {
+        if (r2 <= gmax[gr]) {
+            if (r2 <= gmin[gr]) {
+#pragma unroll
+                for (int j = 4 * gr; j < 4 * gr + 4; ++j)
+                    adj_term<AMP, false, NT>(sbase, r2, base, wsf, shi, T2[j], F4[j], BB[j],
+                                             MK[j]);
+            } else {
+#pragma unroll
+                for (int j = 4 * gr; j < 4 * gr + 4; ++j)
+                    adj_term<AMP, true, NT>(sbase, r2, base, wsf, shi, T2[j], F4[j], BB[j],
+                                            MK[j]);
+            }
+        }
+    }
 }
 
 // Add the windows of one released stage into the data cube (one bulk reduction per window,
-// lanes in parallel) and wait until they have read shared memory.
+// lanes in parallel; a pair's second window follows its first) and wait until they have read
+// shared memory.
 __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
                                           uint32_t smem_abs, int lane) {
     fence_proxy_async_smem();  // the consumers' shared-memory adds -> the async proxy
@@ -133,6 +171,11 @@ __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
         bulk_reduce_add_f32(
             A.data + (static_cast<size_t>(gg.x) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
             smem_abs + rel, 4u * gg.w);
+        const int rb = m.rowb[k];
+        if (rb >= 0)
+            bulk_reduce_add_f32(
+                A.data + (static_cast<size_t>(rb) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
+                smem_abs + rel + 4u * gg.w, 4u * gg.w);
     }
     bulk_commit();
     bulk_wait_read_all();
@@ -257,14 +300,24 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         int* inl_pre = reinterpret_cast<int*>(smem_raw + L.inl_pre);
         float* inl_dx2 = reinterpret_cast<float*>(smem_raw + L.inl_dx2);
         const int n_inl = max(job.i1 - job.i0, 0);
+        // rows of the trace list: the buffer inlines, or the mirror distances d from the centre
+        // inline pc (row d holds inlines pc - d and pc + d; see row_inlines)
+        int pc = -1;
+        if (P.pairable && 2 * P.ns <= P.stage_cap && n_inl > 0) {
+            const int c = job.pos - __ldg(P.il_pos + job.i0);
+            if (c >= 0 && c < n_inl) pc = c;
+        }
+        const int n_rows = pc >= 0 ? max(pc, n_inl - 1 - pc) + 1 : n_inl;
         int total = 0;
         if (S.any && xa <= xb) {
-            for (int base = 0; base < n_inl; base += 32) {
+            for (int base = 0; base < n_rows; base += 32) {
                 const int n = base + lane;
                 int cnt = 0, klo = 0;
                 float dx2 = 0.0f;
-                if (n < n_inl) {
-                    dx2 = inline_dx2(__ldg(P.il_pos + job.i0 + n), job.pos, P.d_il);
+                if (n < n_rows) {
+                    int a, b;
+                    row_inlines(pc, n_inl, n, &a, &b);
+                    dx2 = inline_dx2(__ldg(P.il_pos + job.i0 + a), job.pos, P.d_il);
                     if (dx2 <= S.bmax) {
                         const int K =
                             static_cast<int>(sqrtf(fmaxf(S.bmax - dx2, 0.0f)) * P.inv_dxl) + 2;
@@ -280,10 +333,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                     const int v = __shfl_up_sync(0xffffffffu, incl, o);
                     if (lane >= o) incl += v;
                 }
-                if (n < n_inl) inl_pre[n] = total + incl - cnt;
+                if (n < n_rows) inl_pre[n] = total + incl - cnt;
                 total += __shfl_sync(0xffffffffu, incl, 31);
             }
-            if (lane == 0) inl_pre[n_inl] = total;
+            if (lane == 0) inl_pre[n_rows] = total;
             __syncwarp();
         }
         uint32_t it = 0;
@@ -291,10 +344,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         int f = 0;
         while (f < total && alive) {
             const int idx = f + lane;
-            int ws = 0, size = 0, kc = 0, row = 0;
+            int ws = 0, size = 0, kc = 0, row = 0, rowb = -1, slot_size = 0;
             float dx2 = 0.0f, shi = 0.0f;
             if (idx < total) {
-                int lo = 0, hi = n_inl - 1;
+                int lo = 0, hi = n_rows - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
                     if (inl_pre[mid] <= idx)
@@ -304,10 +357,14 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                 }
                 kc = inl_klo[lo] + (idx - inl_pre[lo]);
                 dx2 = inl_dx2[lo];
-                row = job.i0 + lo;
+                int a, b;
+                row_inlines(pc, n_inl, lo, &a, &b);
+                row = job.i0 + a;
+                rowb = b >= 0 ? job.i0 + b : -1;
                 adj_window(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
+                slot_size = rowb >= 0 ? 2 * size : size;  // a pair's windows are the same
             }
-            int cum = size;
+            int cum = slot_size;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int v = __shfl_up_sync(0xffffffffu, cum, o);
@@ -334,16 +391,24 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                                                       4u * stage * P.stage_cap);
                 for (int k = lane; k < tot / 4; k += 32) z[k] = make_float4(0.f, 0.f, 0.f, 0.f);
                 const uint32_t dst_rel =
-                    L.stage + (static_cast<uint32_t>(stage) * P.stage_cap + (cum - size)) * 4u;
+                    L.stage +
+                    (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) * 4u;
+                const int slot = __popc(nzmask & ((1u << lane) - 1u));
+                const unsigned pm = __reduce_or_sync(
+                    0xffffffffu, take && size > 0 && rowb >= 0 ? (1u << slot) : 0u);
                 if (take && size > 0) {
-                    const int slot = __popc(nzmask & ((1u << lane) - 1u));
                     m.m[slot] = make_int4(kc, __float_as_int(dx2),
                                           static_cast<int>(dst_rel - 4u * ws - kMagic4),
                                           __float_as_int(static_cast<float>(ws)));
                     m.shi[slot] = shi;
                     m.g[slot] = make_int4(row, kc, ws, size);
+                    m.baseb[slot] = static_cast<int>(dst_rel + 4u * size - 4u * ws - kMagic4);
+                    m.rowb[slot] = rowb;
                 }
-                if (lane == 0) m.count = n;
+                if (lane == 0) {
+                    m.count = n;
+                    m.pairmask = pm;
+                }
                 __threadfence_block();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&full[stage]);
@@ -386,28 +451,21 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         const AdjMeta& m = meta[stage];
         const int cnt = m.count;
         if (cnt < 0) break;
+        const unsigned pmask = m.pairmask;
         for (int g = 0; g < cnt; ++g) {
             const int4 md = m.m[g];
             const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
             if (r2 > warpmax) continue;
-            const uint32_t base2 = static_cast<uint32_t>(md.z);
+            uint32_t base[2];
+            base[0] = static_cast<uint32_t>(md.z);
             const float wsf = __int_as_float(md.w);
             const float shi = m.shi[g];
-#pragma unroll
-            for (int gr = 0; gr < 2; ++gr) {
-                if (r2 <= gmax[gr]) {
-                    if (r2 <= gmin[gr]) {
-#pragma unroll
-                        for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                            adj_term<AMP, false>(smem_raw, r2, base2, wsf, shi, T2[j], F4[j],
-                                                 BB[j], MK[j]);
-                    } else {
-#pragma unroll
-                        for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                            adj_term<AMP, true>(smem_raw, r2, base2, wsf, shi, T2[j], F4[j],
-                                                BB[j], MK[j]);
-                    }
-                }
+            if ((pmask >> g) & 1u) {
+                base[1] = static_cast<uint32_t>(m.baseb[g]);
+                adj_visit<AMP, 2>(smem_raw, r2, base, wsf, shi, gmax, gmin, T2, F4, BB, MK);
+            } else {
+                base[1] = 0u;
+                adj_visit<AMP, 1>(smem_raw, r2, base, wsf, shi, gmax, gmin, T2, F4, BB, MK);
             }
         }
         __syncwarp();
