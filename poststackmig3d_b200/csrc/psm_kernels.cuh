@@ -93,7 +93,6 @@ struct StageMeta {
     int pad[3];
     int4 m[kMaxG];    // crossline, dx^2 (bits), window base (smem bytes, see consumers),
                       // window start as float (bits)
-    float shi[kMaxG]; // largest s that stays inside the window
     float sc[kMaxG];  // trace scale (16-bit storage)
     float wend[kMaxG];  // window end as float (read by the debug-bounds build)
     int baseb[kMaxG];   // paired slots: window base of the mirrored trace (see consumers)
@@ -411,40 +410,37 @@ __device__ __forceinline__ bool trace_bounds(const FwdParams& P, const TileStats
 template <int STORE>
 __device__ __forceinline__ void trace_window(const FwdParams& P, const TileStats& S, int xa,
                                              int xb, float dx2, int kc, int* ws_out,
-                                             int* size_out, float* shi_out) {
+                                             int* size_out) {
     constexpr int A = 16 / store_bytes(STORE);
     *ws_out = 0;
     *size_out = 0;
-    *shi_out = 0.0f;
     int lolo, lohi;
     if (!trace_bounds(P, S, xa, xb, dx2, kc, &lolo, &lohi)) return;
     const int ws = lolo & ~(A - 1);
     const int we = (lohi + 1 + A) & ~(A - 1);  // elements [ws, we) cover [lolo, lohi + 1]
     *ws_out = ws;
     *size_out = we - ws;
-    *shi_out = fminf(P.ntm1m, __uint_as_float(__float_as_uint(static_cast<float>(we)) - 1u));
 }
 
 // Staged window of one trace as the consumers see it.
 struct Win {
     float wsf;  // first staged sample (float)
-    float shi;  // largest s whose element is staged, and below n_t - 1
     float wef;  // end of the window (float): the debug-bounds build checks s < wef
     int* err;
 };
 
-// s of a term, kept inside the staged window.  With MASK (some lane of the group may fail the
-// masks) s is clamped: a failing term's s can lie anywhere.  Without MASK every term of the
-// group passes both masks, and trace_window's bounds (two samples of slack, one extra
-// element) put floor(s) inside [ws, we): no clamp is needed.  The debug-bounds build checks
-// that claim and records PSM_DEV_ERR_WINDOW instead of reading outside the window.
-template <bool MASK>
-__device__ __forceinline__ float window_s(float s, const Win& w) {
-    if (MASK) return fminf(fmaxf(s, w.wsf), w.shi);
+// s of a term, kept inside the staged window.  A term that passes both masks needs no clamp:
+// trace_window's bounds (two samples of slack, one extra element) put its floor(s) inside
+// [ws, we).  A term that fails them (ok false, only in groups where some lane may fail) can
+// have its s anywhere: it reads the window's first sample instead, and its value is dropped.
+// The debug-bounds build checks the claim for passing terms and records PSM_DEV_ERR_WINDOW
+// instead of reading outside the window.
+__device__ __forceinline__ float window_s(float s, bool ok, const Win& w) {
+    s = ok ? s : w.wsf;
 #ifdef PSM_DEBUG_BOUNDS
     if (!(s >= w.wsf && s < w.wef)) {
         atomicOr(w.err, PSM_DEV_ERR_WINDOW);
-        return fminf(fmaxf(s, w.wsf), w.shi);
+        return w.wsf;
     }
 #endif
     return s;
@@ -458,15 +454,16 @@ template <bool AMP, bool MASK>
 __device__ __forceinline__ void term_one(const unsigned char* sbase, float r2, uint32_t base2,
                                          const Win& w, float T2, float F4, float BB,
                                          float& ACC) {
+    const bool ok = !MASK || r2 <= BB;                       // both reference masks
     const float t2 = __fmaf_rn(F4, r2, T2);                  // (t / dt)^2
     const float q = rsqrtf(t2);                              // dt / t
-    const float s = window_s<MASK>(t2 * q, w);               // t / dt inside the window
+    const float s = window_s(t2 * q, ok, w);                 // t / dt inside the window
     const float mm = __fadd_rd(s, 8388608.0f);               // 2^23 + floor(s)
     const float fr = s - (mm - 8388608.0f);                  // frac
     const float2 p =
         *reinterpret_cast<const float2*>(sbase + (base2 + (__float_as_uint(mm) << 3)));
     float v = __fmaf_rn(fr, p.y, p.x);                       // simdInterpolate
-    if (MASK) v = r2 <= BB ? v : 0.0f;
+    if (MASK) v = ok ? v : 0.0f;
     if (AMP)
         ACC = __fmaf_rn(v, q, ACC);
     else
@@ -482,11 +479,12 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
         term_one<AMP, MASK>(sbase, r2, base2, w, T2.y, F4.y, BB.y, ACC.y);
         return;
     }
+    const bool ok0 = !MASK || r2 <= BB.x, ok1 = !MASK || r2 <= BB.y;  // reference masks
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
     const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
     float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
-    s.x = window_s<MASK>(s.x, w);                            // inside the staged window
-    s.y = window_s<MASK>(s.y, w);
+    s.x = window_s(s.x, ok0, w);                             // inside the staged window
+    s.y = window_s(s.y, ok1, w);
     const float2 M = make_float2(8388608.0f, 8388608.0f);
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
@@ -497,8 +495,8 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
     float v0 = fmaf(fr.x, p0.y, p0.x);                       // simdInterpolate
     float v1 = fmaf(fr.y, p1.y, p1.x);
     if (MASK) {
-        v0 = r2 <= BB.x ? v0 : 0.0f;
-        v1 = r2 <= BB.y ? v1 : 0.0f;
+        v0 = ok0 ? v0 : 0.0f;
+        v1 = ok1 ? v1 : 0.0f;
     }
     if (AMP)
         ACC = fma2(make_float2(v0, v1), make_float2(q0, q1), ACC);
@@ -515,11 +513,12 @@ __device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
                                            const uint32_t (&base)[2], const Win& w,
                                            const float2& T2, const float2& F4, const float2& BB,
                                            float2& ACC) {
+    const bool ok0 = !MASK || r2 <= BB.x, ok1 = !MASK || r2 <= BB.y;  // reference masks
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
     const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
     float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
-    s.x = window_s<MASK>(s.x, w);                            // inside the staged windows
-    s.y = window_s<MASK>(s.y, w);
+    s.x = window_s(s.x, ok0, w);                             // inside the staged windows
+    s.y = window_s(s.y, ok1, w);
     const float2 M = make_float2(8388608.0f, 8388608.0f);
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
@@ -533,8 +532,8 @@ __device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
     }
     float2 v = make_float2(fmaf(fr.x, a0.y, a0.x), fmaf(fr.y, a1.y, a1.x));
     if (MASK) {
-        v.x = r2 <= BB.x ? v.x : 0.0f;
-        v.y = r2 <= BB.y ? v.y : 0.0f;
+        v.x = ok0 ? v.x : 0.0f;
+        v.y = ok1 ? v.y : 0.0f;
     }
     if (AMP)
         ACC = fma2(v, make_float2(q0, q1), ACC);
@@ -558,11 +557,12 @@ template <bool AMP, bool MASK, int STORE>
 __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2, uint32_t base2,
                                             const Win& w, float sc, const float2& T2,
                                             const float2& F4, const float2& BB, float2& ACC) {
+    const bool ok0 = !MASK || r2 <= BB.x, ok1 = !MASK || r2 <= BB.y;  // reference masks
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
     const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
     float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
-    s.x = window_s<MASK>(s.x, w);                            // inside the staged window
-    s.y = window_s<MASK>(s.y, w);
+    s.x = window_s(s.x, ok0, w);                             // inside the staged window
+    s.y = window_s(s.y, ok1, w);
     const float2 M = make_float2(8388608.0f, 8388608.0f);
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
@@ -574,8 +574,8 @@ __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2
     const float2 a = make_float2(p0.x, p1.x);
     float2 v = fma2(fr, sub2(make_float2(p0.y, p1.y), a), a);  // simdInterpolate
     if (MASK) {
-        v.x = r2 <= BB.x ? v.x : 0.0f;
-        v.y = r2 <= BB.y ? v.y : 0.0f;
+        v.x = ok0 ? v.x : 0.0f;
+        v.y = ok1 ? v.y : 0.0f;
     }
     if (AMP)
         ACC = fma2(v, mul2(make_float2(q0, q1), make_float2(sc, sc)), ACC);
@@ -590,11 +590,12 @@ __device__ __forceinline__ void term_pair2_16(const unsigned char* sbase, float 
                                               uint32_t base2a, uint32_t base2b, const Win& w,
                                               float sca, float scb, const float2& T2,
                                               const float2& F4, const float2& BB, float2& ACC) {
+    const bool ok0 = !MASK || r2 <= BB.x, ok1 = !MASK || r2 <= BB.y;  // reference masks
     const float2 t2 = fma2(F4, make_float2(r2, r2), T2);     // (t / dt)^2
     const float q0 = rsqrtf(t2.x), q1 = rsqrtf(t2.y);        // dt / t
     float2 s = mul2(t2, make_float2(q0, q1));                // t / dt
-    s.x = window_s<MASK>(s.x, w);                            // inside the staged windows
-    s.y = window_s<MASK>(s.y, w);
+    s.x = window_s(s.x, ok0, w);                             // inside the staged windows
+    s.y = window_s(s.y, ok1, w);
     const float2 M = make_float2(8388608.0f, 8388608.0f);
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
@@ -608,8 +609,8 @@ __device__ __forceinline__ void term_pair2_16(const unsigned char* sbase, float 
     const float2 vb = fma2(fr, sub2(make_float2(b0.y, b1.y), lb), lb);
     float2 v = fma2(va, make_float2(sca, sca), mul2(vb, make_float2(scb, scb)));
     if (MASK) {
-        v.x = r2 <= BB.x ? v.x : 0.0f;
-        v.y = r2 <= BB.y ? v.y : 0.0f;
+        v.x = ok0 ? v.x : 0.0f;
+        v.y = ok1 ? v.y : 0.0f;
     }
     if (AMP)
         ACC = fma2(v, make_float2(q0, q1), ACC);
@@ -640,7 +641,7 @@ __device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2,
 // group passes, without masks where every lane of the group (or of the tile) passes.
 template <bool AMP, bool PACKED, int GB, int J, int STORE, int NT>
 __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
-                                           const uint32_t (&base)[2], Win w, const float* shi,
+                                           const uint32_t (&base)[2], const Win& w,
                                            float sc, float scb,
                                            float gminall, const float (&gmax)[J / GB],
                                            const float (&gmin)[J / GB], const float2 (&T2)[J / 2],
@@ -655,7 +656,6 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
                                                       T2[p], F4[p], BB[p], SUM[p]);
         return;
     }
-    w.shi = *shi;
 #pragma unroll
     for (int gr = 0; gr < NG; ++gr) {
         if (r2 <= gmax[gr]) {
@@ -862,7 +862,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         while (f < total && alive) {
             const int idx = f + lane;
             int ws = 0, size = 0, kc = 0, row = 0, rowb = -1, slot_size = 0;
-            float dx2 = 0.0f, shi = 0.0f, sc = 1.0f, scb = 1.0f;
+            float dx2 = 0.0f, sc = 1.0f, scb = 1.0f;
             if (idx < total) {
                 // row of flat slot idx: the last n with inl_pre[n] <= idx
                 int lo = 0, hi = n_rows - 1;
@@ -879,7 +879,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                 row_inlines(pc, n_inl, lo, &a, &b);
                 row = job.i0 + a;
                 rowb = b >= 0 ? job.i0 + b : -1;
-                trace_window<STORE>(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
+                trace_window<STORE>(P, S, xa, xb, dx2, kc, &ws, &size);
                 if (STORE != kStoreF32 && size > 0) {
                     sc = __ldg(P.scales + static_cast<size_t>(row) * P.n_cx + kc);
                     if (rowb >= 0) scb = __ldg(P.scales + static_cast<size_t>(rowb) * P.n_cx + kc);
@@ -922,7 +922,6 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     m.m[slot] = make_int4(kc, __float_as_int(dx2),
                                           static_cast<int>(dst_rel - EB * ws - MAGIC),
                                           __float_as_int(static_cast<float>(ws)));
-                    m.shi[slot] = shi;
                     m.sc[slot] = sc;
                     m.wend[slot] = static_cast<float>(ws + size);
                     m.baseb[slot] = static_cast<int>(dst_rel + EB * size - EB * ws - MAGIC);
@@ -1006,10 +1005,8 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             Win w;
             w.wsf = __int_as_float(md.w);
 #ifdef PSM_DEBUG_BOUNDS
-            w.shi = m.shi[g];
             w.wef = m.wend[g];
 #else
-            w.shi = 0.0f;  // read by visit_slot, where a clamp needs it
             w.wef = 0.0f;
 #endif
             w.err = P.err;
@@ -1017,13 +1014,12 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             if (PAIRS && ((pmask >> g) & 1u)) {
                 base[1] = static_cast<uint32_t>(m.baseb[g]);
                 visit_slot<AMP, PACKED, GB, J, STORE, 2>(
-                    smem_raw, r2, base, w, &m.shi[g], sc, STORE == kStoreF32 ? 1.0f : m.scb[g],
+                    smem_raw, r2, base, w, sc, STORE == kStoreF32 ? 1.0f : m.scb[g],
                     gminall, gmax, gmin, T2, F4, BB, SUM);
             } else {
                 base[1] = 0u;
-                visit_slot<AMP, PACKED, GB, J, STORE, 1>(smem_raw, r2, base, w, &m.shi[g], sc,
-                                                         1.0f, gminall, gmax, gmin, T2, F4, BB,
-                                                         SUM);
+                visit_slot<AMP, PACKED, GB, J, STORE, 1>(smem_raw, r2, base, w, sc, 1.0f,
+                                                         gminall, gmax, gmin, T2, F4, BB, SUM);
             }
         }
         if (KAHAN) {  // ACC += PART, compensated
