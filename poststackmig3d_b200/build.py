@@ -76,7 +76,7 @@ def build_host(force: bool = False) -> str:
 
 
 def build(force: bool = False, debug_bounds: bool = False) -> None:
-    """debug_bounds: the forward kernel checks that every unclamped sample index lies inside
+    """debug_bounds: the forward kernel checks that every sample index it reads lies inside
     its staged window and reports PSM_ERR_DEVICE instead of reading outside it (slower;
     for validation runs)."""
     build_cuda(force, ["-DPSM_DEBUG_BOUNDS"] if debug_bounds else ())
