@@ -33,7 +33,6 @@ struct AdjMeta {
     unsigned pairmask; // bit k: slot k holds a mirrored pair (a second window after the first)
     int pad[2];
     int4 m[kMaxG];     // crossline, dx^2 (bits), window base (smem bytes), window start (f32)
-    float shi[kMaxG];  // largest s whose lo and lo + 1 stay inside the window
     int4 g[kMaxG];     // flush: cube row, crossline, window start, window length (samples)
     int baseb[kMaxG];  // paired slots: window base of the mirrored trace
     int rowb[kMaxG];   // paired slots: cube row of the mirrored trace (-1: none)
@@ -92,32 +91,33 @@ __device__ __forceinline__ void bulk_wait_all() {
 
 // Producer: the fp32 window of trace (dx2, kc): samples [ws, we) cover lo and lo + 1 of every
 // passing term of the tile; ws and we multiples of 4 (16-byte bulk-copy granularity).
+// trace_bounds puts lo of a passing term in [lolo, lohi + 1] (the extra sample for a fast s
+// that rounds up across lohi + 1), and the consumers keep s below n_t - 1, so lo + 1 <=
+// min(lohi + 2, n_t - 1): the window covers samples up to lohi + 2, or to the row's end.
 __device__ __forceinline__ void adj_window(const FwdParams& P, const TileStats& S, int xa,
                                            int xb, float dx2, int kc, int* ws_out,
-                                           int* size_out, float* shi_out) {
+                                           int* size_out) {
     *ws_out = 0;
     *size_out = 0;
-    *shi_out = 0.0f;
     int lolo, lohi;
     if (!trace_bounds(P, S, xa, xb, dx2, kc, &lolo, &lohi)) return;
     const int ws = lolo & ~3;
-    // sample lohi + 1 <= n_t - 1 included; ns is a multiple of 8, so we <= ns
-    const int we = min((lohi + 2 + 3) & ~3, P.ns);
+    const int we = min((lohi + 3 + 3) & ~3, P.ns);  // ns >= n_t, a multiple of 8
     *ws_out = ws;
     *size_out = we - ws;
-    // lo <= we - 2  <=>  s < we - 1
-    *shi_out = fminf(P.ntm1m, __uint_as_float(__float_as_uint(static_cast<float>(we - 1)) - 1u));
 }
 
 // One term of the transpose (scalar FP32) for the NT traces of a slot (a mirrored pair: the
-// same r^2): the forward's s, frac and q, then two atomic adds into each trace's window.
+// same r^2): the forward's s, frac and q, then two atomic adds into each trace's window.  A
+// failing term (MASK) returns before touching memory; a passing term's lo lies in its window
+// (adj_window), with s held below n_t - 1 (smax) so that lo + 1 stays on the trace.
 template <bool AMP, bool MASK, int NT>
 __device__ __forceinline__ void adj_term(unsigned char* sbase, float r2,
-                                         const uint32_t (&base)[2], float wsf, float shi,
+                                         const uint32_t (&base)[2], float smax,
                                          float T2, float F4, float BB, float MK) {
     const float t2 = __fmaf_rn(F4, r2, T2);
     const float q = rsqrtf(t2);
-    const float s = fminf(fmaxf(t2 * q, wsf), shi);
+    const float s = fminf(t2 * q, smax);
     const float mm = __fadd_rd(s, 8388608.0f);
     const float fr = s - (mm - 8388608.0f);
     if (MASK && !(r2 <= BB)) return;
@@ -137,7 +137,7 @@ __device__ __forceinline__ void adj_term(unsigned char* sbase, float r2,
 // where every lane of the group passes.
 template <bool AMP, int NT>
 __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2,
-                                          const uint32_t (&base)[2], float wsf, float shi,
+                                          const uint32_t (&base)[2], float smax,
                                           const float (&gmax)[2], const float (&gmin)[2],
                                           const float (&T2)[kJ], const float (&F4)[kJ],
                                           const float (&BB)[kJ], const float (&MK)[kJ]) {
@@ -147,12 +147,12 @@ __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2,
             if (r2 <= gmin[gr]) {
 #pragma unroll
                 for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, false, NT>(sbase, r2, base, wsf, shi, T2[j], F4[j], BB[j],
+                    adj_term<AMP, false, NT>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
                                              MK[j]);
             } else {
 #pragma unroll
                 for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, true, NT>(sbase, r2, base, wsf, shi, T2[j], F4[j], BB[j],
+                    adj_term<AMP, true, NT>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
                                             MK[j]);
             }
         }
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         while (f < total && alive) {
             const int idx = f + lane;
             int ws = 0, size = 0, kc = 0, row = 0, rowb = -1, slot_size = 0;
-            float dx2 = 0.0f, shi = 0.0f;
+            float dx2 = 0.0f;
             if (idx < total) {
                 int lo = 0, hi = n_rows - 1;
                 while (lo < hi) {
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                 row_inlines(pc, n_inl, lo, &a, &b);
                 row = job.i0 + a;
                 rowb = b >= 0 ? job.i0 + b : -1;
-                adj_window(P, S, xa, xb, dx2, kc, &ws, &size, &shi);
+                adj_window(P, S, xa, xb, dx2, kc, &ws, &size);
                 slot_size = rowb >= 0 ? 2 * size : size;  // a pair's windows are the same
             }
             int cum = slot_size;
@@ -400,7 +400,6 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                     m.m[slot] = make_int4(kc, __float_as_int(dx2),
                                           static_cast<int>(dst_rel - 4u * ws - kMagic4),
                                           __float_as_int(static_cast<float>(ws)));
-                    m.shi[slot] = shi;
                     m.g[slot] = make_int4(row, kc, ws, size);
                     m.baseb[slot] = static_cast<int>(dst_rel + 4u * size - 4u * ws - kMagic4);
                     m.rowb[slot] = rowb;
@@ -458,14 +457,12 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
             if (r2 > warpmax) continue;
             uint32_t base[2];
             base[0] = static_cast<uint32_t>(md.z);
-            const float wsf = __int_as_float(md.w);
-            const float shi = m.shi[g];
             if ((pmask >> g) & 1u) {
                 base[1] = static_cast<uint32_t>(m.baseb[g]);
-                adj_visit<AMP, 2>(smem_raw, r2, base, wsf, shi, gmax, gmin, T2, F4, BB, MK);
+                adj_visit<AMP, 2>(smem_raw, r2, base, P.ntm1m, gmax, gmin, T2, F4, BB, MK);
             } else {
                 base[1] = 0u;
-                adj_visit<AMP, 1>(smem_raw, r2, base, wsf, shi, gmax, gmin, T2, F4, BB, MK);
+                adj_visit<AMP, 1>(smem_raw, r2, base, P.ntm1m, gmax, gmin, T2, F4, BB, MK);
             }
         }
         __syncwarp();

@@ -39,6 +39,7 @@ constexpr int kJ = 8;           // 32-sample blocks per consumer lane
 constexpr int kTT = 32 * kJ;    // output samples per CTA
 constexpr int kStages = 2;      // TMA ring depth
 constexpr int kMaxG = 32;       // traces per ring stage
+static_assert(kTX % 4 == 0, "per-slot r^2 rows are stored as float4");
 constexpr int kStageCapMin = 6144;          // samples (8 B each) per ring stage, at least
 constexpr unsigned kWaitLimit = 1u << 26;   // bounded mbarrier polls
 
@@ -97,6 +98,7 @@ struct StageMeta {
     float wend[kMaxG];  // window end as float (read by the debug-bounds build)
     int baseb[kMaxG];   // paired slots: window base of the mirrored trace (see consumers)
     float scb[kMaxG];   // paired slots, 16-bit storage: the mirrored trace's scale
+    float r2[kMaxG][kTX];  // r^2 of the slot's trace(s) to each consumer warp's crossline
     unsigned pairmask;  // bit g: slot g holds a mirrored pair of traces
     int pad2[3];
 };
@@ -926,6 +928,16 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     m.wend[slot] = static_cast<float>(ws + size);
                     m.baseb[slot] = static_cast<int>(dst_rel + EB * size - EB * ws - MAGIC);
                     m.scb[slot] = scb;
+                    // r^2 to each consumer warp's output crossline, with the consumers'
+                    // arithmetic (trace_r2), so that each warp reads it instead
+                    float rr[kTX];
+#pragma unroll
+                    for (int w = 0; w < kTX; ++w)
+                        rr[w] = trace_r2(kc - (x0 + w + P.xoff), P.d_xl, dx2);
+                    float4* r2d = reinterpret_cast<float4*>(&m.r2[slot][0]);
+#pragma unroll
+                    for (int w = 0; w < kTX; w += 4)
+                        r2d[w / 4] = make_float4(rr[w], rr[w + 1], rr[w + 2], rr[w + 3]);
                 }
                 if (lane == 0) {
                     m.count = n;
@@ -997,9 +1009,9 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         }
         const unsigned pmask = PAIRS ? m.pairmask : 0u;
         for (int g = 0; g < cnt; ++g) {
-            const int4 md = m.m[g];
-            const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
+            const float r2 = m.r2[g][warp - 1];
             if (r2 > warpmax) continue;
+            const int4 md = m.m[g];
             uint32_t base[2];
             base[0] = static_cast<uint32_t>(md.z);
             Win w;
