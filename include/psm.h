@@ -99,9 +99,10 @@ int psm_forward(psm_ctx *ctx, float *image);
 
 /* Forward migration from host buffers in one call: traces and vrms [n_il][n_xl][n_t] (host)
  * in, image [n_oi][n_ox][n_t] (host) out.  Pipelined: inline blocks upload on a copy stream,
- * the output inlines whose buffers are resident migrate while later blocks upload, and image
- * rows return on a third stream while later output inlines migrate (pinned host buffers let
- * the copies overlap).  Leaves the traces and Vrms resident, as psm_set_traces/_vrms. */
+ * the output inlines whose buffers and Vrms rows are resident migrate (on two alternating
+ * compute streams) while later blocks upload, and image rows return on another stream while
+ * later output inlines migrate (pinned host buffers let the copies overlap).  Leaves the
+ * traces and Vrms resident, as psm_set_traces/_vrms. */
 int psm_forward_host(psm_ctx *ctx, const float *traces, const float *vrms, float *image);
 
 /* Same as psm_forward, leaving the image in device memory owned by ctx (enqueued on the ctx

@@ -385,8 +385,10 @@ struct psm_ctx {
     int seg_rec_bytes = 0;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copied = nullptr;
-    // psm_forward_host: the device-to-host stream and the jobs in wave order
+    // psm_forward_host: the device-to-host stream, a second compute stream and the jobs in
+    // wave order
     cudaStream_t d2h_stream = nullptr;
+    cudaStream_t aux_stream = nullptr;
     DevBuf d_jobs_waves;
 };
 
@@ -479,6 +481,7 @@ int psm_destroy(psm_ctx* c) {
     if (c->copied) cudaEventDestroy(c->copied);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->d2h_stream) cudaStreamDestroy(c->d2h_stream);
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     c->d_jobs_waves.release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -908,38 +911,62 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
     cudaSetDevice(c->device);
     const psm_geom& g = c->g;
     cudaStream_t s = c->stream;
-    if (!c->copy_stream)
-        PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-    if (!c->d2h_stream)
-        PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking));
-    // input inlines in n_blocks consecutive blocks, uploaded in order.  Few and large: a CTA
-    // of a full-size cube runs for milliseconds, so every extra launch costs a tail of idle
-    // SMs, and an output inline's buffer spans much of the cube anyway.
-    const int n_blocks = std::min(g.n_il, 4);
+    for (cudaStream_t* t : {&c->copy_stream, &c->d2h_stream, &c->aux_stream})
+        if (!*t) PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(t, cudaStreamNonBlocking));
+    // Inputs go up in blocks of consecutive inlines: trace block b (then its pair cube or 16-bit
+    // words, built on the copy stream), and Vrms block v once the trace blocks that the output
+    // inlines of block v read are up (an output inline needs its whole buffer, which reaches
+    // about m_il + pad_il inlines ahead, but only its own Vrms row).  A job runs in the wave of
+    // the first upload after which its buffer and Vrms row are resident.  Waves alternate
+    // between two compute streams, so that one launch's tail of finishing CTAs overlaps the
+    // next launch instead of idling SMs; the last wave is cut in two so that most of its rows
+    // stream back while the rest migrate.
+    const int n_blocks = std::min(g.n_il, 8);
     auto block_end = [&](int b) { return static_cast<int>(int64_t(b + 1) * g.n_il / n_blocks); };
-    // a job runs in the wave of the first block after which its buffer and Vrms row are
-    // resident; the last wave is cut in two so that most of its rows stream back while the
-    // rest migrate
+    auto block_of = [&](int inl) {  // block holding inline inl
+        int b = 0;
+        while (block_end(b) <= inl) ++b;
+        return b;
+    };
     const int n_jobs = static_cast<int>(c->jobs.size());
-    std::vector<std::vector<int>> wave(n_blocks);
+    // Vrms block v goes up after trace block lead[v]: the last trace block any job of v reads
+    std::vector<int> lead(n_blocks, 0);
     for (int k = 0; k < n_jobs; ++k) {
         const Job& j = c->jobs[k];
-        const int need = std::max(j.i1, j.vrow + 1);
-        int b = 0;
-        while (block_end(b) < need) ++b;
-        wave[b].push_back(k);
+        const int v = block_of(j.vrow);
+        lead[v] = std::max(lead[v], block_of(std::max(j.i1, 1) - 1));
     }
+    for (int v = 1; v < n_blocks; ++v) lead[v] = std::max(lead[v], lead[v - 1]);
+    std::vector<std::pair<int, int>> units;  // upload order: (0 traces / 1 Vrms, block)
+    std::vector<int> t_unit(n_blocks), v_unit(n_blocks);
+    for (int b = 0, v = 0; b < n_blocks; ++b) {
+        t_unit[b] = static_cast<int>(units.size());
+        units.emplace_back(0, b);
+        for (; v < n_blocks && lead[v] <= b; ++v) {
+            v_unit[v] = static_cast<int>(units.size());
+            units.emplace_back(1, v);
+        }
+    }
+    const int n_units = static_cast<int>(units.size());
+    std::vector<std::vector<int>> wave(n_units);
+    for (int k = 0; k < n_jobs; ++k) {
+        const Job& j = c->jobs[k];
+        const int u = std::max(t_unit[block_of(std::max(j.i1, 1) - 1)], v_unit[block_of(j.vrow)]);
+        wave[u].push_back(k);
+    }
+    int last = n_units - 1;
+    while (last > 0 && wave[last].empty()) --last;
     std::vector<Job> order;
-    std::vector<std::pair<int, int>> chunks;  // (first job in order, count), after block b
-    std::vector<int> chunk_block;
-    for (int b = 0; b < n_blocks; ++b) {
-        const size_t w = wave[b].size();
-        const size_t chunk_jobs = b == n_blocks - 1 && w >= 16 ? (w * 3 + 3) / 4 : w;
+    std::vector<std::pair<int, int>> chunks;  // (first job in order, count)
+    std::vector<int> chunk_unit;              // upload the chunk waits for
+    for (int u = 0; u < n_units; ++u) {
+        const size_t w = wave[u].size();
+        const size_t chunk_jobs = u == last && w >= 16 ? (w * 3 + 3) / 4 : std::max<size_t>(w, 1);
         for (size_t i = 0; i < w; i += chunk_jobs) {
             const int n = static_cast<int>(std::min<size_t>(chunk_jobs, w - i));
             chunks.emplace_back(static_cast<int>(order.size()), n);
-            chunk_block.push_back(b);
-            for (int t = 0; t < n; ++t) order.push_back(c->jobs[wave[b][i + t]]);
+            chunk_unit.push_back(u);
+            for (int t = 0; t < n; ++t) order.push_back(c->jobs[wave[u][i + t]]);
         }
     }
     // rows each job's image fills: its own, then the rows that repeat it
@@ -949,7 +976,8 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
     PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_jobs_waves.p, order.data(), order.size() * sizeof(Job),
                                         cudaMemcpyHostToDevice, s));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), s));
-    std::vector<cudaEvent_t> ev(n_blocks + chunks.size(), nullptr);
+    // events: one per upload, one per chunk, the start and the second stream's end
+    std::vector<cudaEvent_t> ev(n_units + chunks.size() + 2, nullptr);
     for (auto& e : ev) {
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
             for (auto& d : ev)
@@ -963,67 +991,82 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
             for (auto& d : e) cudaEventDestroy(d);
         }
     } guard{ev};
-    // the copy stream starts after the ctx stream's earlier work (jobs, error word)
-    PSM_CUDA_TRY(c->st, cudaEventRecord(ev[0], s));
-    PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, ev[0], 0));
+    cudaEvent_t ev_start = ev[n_units + chunks.size()], ev_aux = ev[n_units + chunks.size() + 1];
+    // the copy and second compute streams start after the ctx stream's earlier work (jobs,
+    // error word)
+    PSM_CUDA_TRY(c->st, cudaEventRecord(ev_start, s));
+    PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, ev_start, 0));
+    PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->aux_stream, ev_start, 0));
     const size_t per_il = static_cast<size_t>(g.n_xl) * g.n_t;
-    for (int b = 0; b < n_blocks; ++b) {
+    for (int u = 0; u < n_units; ++u) {
+        const int b = units[u].second;
         const int lo = b ? block_end(b - 1) : 0, hi = block_end(b);
-        const size_t rows = static_cast<size_t>(hi - lo) * g.n_xl;
-        PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.as<float>() + size_t(lo) * g.n_xl * c->ns,
-                                              c->ns * sizeof(float), traces + lo * per_il,
-                                              g.n_t * sizeof(float), g.n_t * sizeof(float), rows,
-                                              cudaMemcpyHostToDevice, c->copy_stream));
-        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.as<float>() + lo * per_il, vrms + lo * per_il,
-                                            rows * g.n_t * sizeof(float), cudaMemcpyHostToDevice,
-                                            c->copy_stream));
-        PSM_CUDA_TRY(c->st, cudaEventRecord(ev[b], c->copy_stream));
+        const size_t r0 = size_t(lo) * g.n_xl, rows = size_t(hi - lo) * g.n_xl;
+        cudaStream_t cs = c->copy_stream;
+        if (units[u].first == 0) {
+            PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.as<float>() + r0 * c->ns,
+                                                  c->ns * sizeof(float), traces + lo * per_il,
+                                                  g.n_t * sizeof(float), g.n_t * sizeof(float),
+                                                  rows, cudaMemcpyHostToDevice, cs));
+            if (c->store == psm::kStoreF32)
+                PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>() + r0 * c->ns,
+                                                c->pairs.as<float2>() + r0 * c->ns, rows, c->ns,
+                                                cs));
+            else
+                PSM_CUDA_TRY(c->st, quantize(c->data.as<float>() + r0 * c->ns,
+                                             c->words.as<uint32_t>() + r0 * c->ns,
+                                             c->scales.as<float>() + r0, rows, c->ns, c->store,
+                                             cs));
+        } else {
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.as<float>() + lo * per_il,
+                                                vrms + lo * per_il, rows * g.n_t * sizeof(float),
+                                                cudaMemcpyHostToDevice, cs));
+        }
+        PSM_CUDA_TRY(c->st, cudaEventRecord(ev[u], cs));
     }
     const size_t row = static_cast<size_t>(g.n_ox) * g.n_t;
     FwdParams P = volume_params(c);
-    size_t k = 0;
-    for (int b = 0; b < n_blocks; ++b) {
-        const int lo = b ? block_end(b - 1) : 0, hi = block_end(b);
-        const size_t r0 = size_t(lo) * g.n_xl, rows = size_t(hi - lo) * g.n_xl;
-        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(s, ev[b], 0));
-        if (c->store == psm::kStoreF32)
-            PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>() + r0 * c->ns,
-                                            c->pairs.as<float2>() + r0 * c->ns, rows, c->ns, s));
-        else
-            PSM_CUDA_TRY(c->st, quantize(c->data.as<float>() + r0 * c->ns,
-                                         c->words.as<uint32_t>() + r0 * c->ns,
-                                         c->scales.as<float>() + r0, rows, c->ns, c->store, s));
-        for (; k < chunks.size() && chunk_block[k] == b; ++k) {
-            FwdParams Q = P;
-            Q.jobs = c->d_jobs_waves.as<Job>() + chunks[k].first;
-            PSM_CUDA_TRY(c->st, launch_fwd(Q, chunks[k].second, g.amp_correction != 0,
-                                           c->variant, s, c->store, g.compensated != 0));
-            std::vector<int> out_rows;
-            for (int t = 0; t < chunks[k].second; ++t) {
-                const int r = order[chunks[k].first + t].row;
-                out_rows.push_back(r);
-                for (int d : dup[r]) {  // padded output inlines repeat the edge inline
-                    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.as<float>() + d * row,
-                                                        c->image.as<float>() + r * row,
-                                                        row * sizeof(float),
-                                                        cudaMemcpyDeviceToDevice, s));
-                    out_rows.push_back(d);
-                }
-            }
-            cudaEvent_t done = ev[n_blocks + k];
-            PSM_CUDA_TRY(c->st, cudaEventRecord(done, s));
-            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, done, 0));
-            std::sort(out_rows.begin(), out_rows.end());
-            for (size_t i = 0; i < out_rows.size();) {  // runs of consecutive rows
-                size_t e = i + 1;
-                while (e < out_rows.size() && out_rows[e] == out_rows[e - 1] + 1) ++e;
-                PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + out_rows[i] * row,
-                                                    c->image.as<float>() + out_rows[i] * row,
-                                                    (e - i) * row * sizeof(float),
-                                                    cudaMemcpyDeviceToHost, c->d2h_stream));
-                i = e;
+    bool aux_used = false;
+    for (size_t k = 0; k < chunks.size(); ++k) {
+        cudaStream_t cs = (k % 2 == 0) ? s : c->aux_stream;
+        aux_used = aux_used || cs != s;
+        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(cs, ev[chunk_unit[k]], 0));
+        FwdParams Q = P;
+        Q.jobs = c->d_jobs_waves.as<Job>() + chunks[k].first;
+        PSM_CUDA_TRY(c->st, launch_fwd(Q, chunks[k].second, g.amp_correction != 0, c->variant,
+                                       cs, c->store, g.compensated != 0));
+        std::vector<int> out_rows;
+        for (int t = 0; t < chunks[k].second; ++t) {
+            const int r = order[chunks[k].first + t].row;
+            out_rows.push_back(r);
+            for (int d : dup[r]) {  // padded output inlines repeat the edge inline
+                PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.as<float>() + d * row,
+                                                    c->image.as<float>() + r * row,
+                                                    row * sizeof(float),
+                                                    cudaMemcpyDeviceToDevice, cs));
+                out_rows.push_back(d);
             }
         }
+        cudaEvent_t done = ev[n_units + k];
+        PSM_CUDA_TRY(c->st, cudaEventRecord(done, cs));
+        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, done, 0));
+        std::sort(out_rows.begin(), out_rows.end());
+        for (size_t i = 0; i < out_rows.size();) {  // runs of consecutive rows
+            size_t e = i + 1;
+            while (e < out_rows.size() && out_rows[e] == out_rows[e - 1] + 1) ++e;
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + out_rows[i] * row,
+                                                c->image.as<float>() + out_rows[i] * row,
+                                                (e - i) * row * sizeof(float),
+                                                cudaMemcpyDeviceToHost, c->d2h_stream));
+            i = e;
+        }
+    }
+    // the ctx stream's later work follows both compute streams and the uploads
+    PSM_CUDA_TRY(c->st, cudaEventRecord(ev_aux, aux_used ? c->aux_stream : c->copy_stream));
+    PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(s, ev_aux, 0));
+    if (aux_used) {
+        PSM_CUDA_TRY(c->st, cudaEventRecord(ev_start, c->copy_stream));
+        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(s, ev_start, 0));
     }
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
