@@ -92,15 +92,12 @@ struct FwdParams {
 struct StageMeta {
     int count;        // traces in this stage, -1 = end of stream
     int pad[3];
-    int4 m[kMaxG];    // crossline, dx^2 (bits), window base (smem bytes, see consumers),
-                      // window start as float (bits)
+    int4 m[kMaxG];    // window base (smem bytes, see consumers), window start as float
+                      // (bits), the mirrored trace's window base, 1 for a mirrored pair
     float sc[kMaxG];  // trace scale (16-bit storage)
     float wend[kMaxG];  // window end as float (read by the debug-bounds build)
-    int baseb[kMaxG];   // paired slots: window base of the mirrored trace (see consumers)
     float scb[kMaxG];   // paired slots, 16-bit storage: the mirrored trace's scale
     float r2[kMaxG][kTX];  // r^2 of the slot's trace(s) to each consumer warp's crossline
-    unsigned pairmask;  // bit g: slot g holds a mirrored pair of traces
-    int pad2[3];
 };
 
 struct TileStats {
@@ -915,18 +912,17 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) * EB;
                 const uint32_t dst = stage0 + (dst_rel - L.stage);
                 const int slot = __popc(nzmask & ((1u << lane) - 1u));
-                const unsigned pm = __reduce_or_sync(
-                    0xffffffffu, take && size > 0 && rowb >= 0 ? (1u << slot) : 0u);
                 if (take && size > 0) {
                     // consumers find sample n of the window at byte
                     // base2 + (bits(2^23 + n) << log2(EB)) from the shared-memory base (32-bit
-                    // wrap-around): base2 = dst_rel - EB ws - (0x4B000000 << log2(EB))
-                    m.m[slot] = make_int4(kc, __float_as_int(dx2),
-                                          static_cast<int>(dst_rel - EB * ws - MAGIC),
-                                          __float_as_int(static_cast<float>(ws)));
+                    // wrap-around): base2 = dst_rel - EB ws - (0x4B000000 << log2(EB)); a
+                    // pair's second window follows its first
+                    m.m[slot] = make_int4(static_cast<int>(dst_rel - EB * ws - MAGIC),
+                                          __float_as_int(static_cast<float>(ws)),
+                                          static_cast<int>(dst_rel + EB * size - EB * ws - MAGIC),
+                                          rowb >= 0 ? 1 : 0);
                     m.sc[slot] = sc;
                     m.wend[slot] = static_cast<float>(ws + size);
-                    m.baseb[slot] = static_cast<int>(dst_rel + EB * size - EB * ws - MAGIC);
                     m.scb[slot] = scb;
                     // r^2 to each consumer warp's output crossline, with the consumers'
                     // arithmetic (trace_r2), so that each warp reads it instead
@@ -939,10 +935,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     for (int w = 0; w < kTX; w += 4)
                         r2d[w / 4] = make_float4(rr[w], rr[w + 1], rr[w + 2], rr[w + 3]);
                 }
-                if (lane == 0) {
-                    m.count = n;
-                    m.pairmask = pm;
-                }
+                if (lane == 0) m.count = n;
                 __threadfence_block();
                 __syncwarp();
                 if (lane == 0)
@@ -1007,15 +1000,14 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
 #pragma unroll
             for (int p = 0; p < J / 2; ++p) PART[p] = make_float2(0.0f, 0.0f);
         }
-        const unsigned pmask = PAIRS ? m.pairmask : 0u;
         for (int g = 0; g < cnt; ++g) {
             const float r2 = m.r2[g][warp - 1];
             if (r2 > warpmax) continue;
             const int4 md = m.m[g];
             uint32_t base[2];
-            base[0] = static_cast<uint32_t>(md.z);
+            base[0] = static_cast<uint32_t>(md.x);
             Win w;
-            w.wsf = __int_as_float(md.w);
+            w.wsf = __int_as_float(md.y);
 #ifdef PSM_DEBUG_BOUNDS
             w.wef = m.wend[g];
 #else
@@ -1023,8 +1015,8 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
 #endif
             w.err = P.err;
             const float sc = STORE == kStoreF32 ? 1.0f : m.sc[g];
-            if (PAIRS && ((pmask >> g) & 1u)) {
-                base[1] = static_cast<uint32_t>(m.baseb[g]);
+            if (PAIRS && md.w) {
+                base[1] = static_cast<uint32_t>(md.z);
                 visit_slot<AMP, PACKED, GB, J, STORE, 2>(
                     smem_raw, r2, base, w, sc, STORE == kStoreF32 ? 1.0f : m.scb[g],
                     gminall, gmax, gmin, T2, F4, BB, SUM);
