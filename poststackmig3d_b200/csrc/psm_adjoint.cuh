@@ -30,12 +30,12 @@ struct AdjParams {
 
 struct AdjMeta {
     int count;         // slots in this stage, -1 = end of stream
-    unsigned pairmask; // bit k: slot k holds a mirrored pair (a second window after the first)
-    int pad[2];
-    int4 m[kMaxG];     // crossline, dx^2 (bits), window base (smem bytes), window start (f32)
+    int pad[3];
+    int4 m[kMaxG];     // window base (smem bytes), the mirrored trace's window base (a pair's
+                       // second window follows its first), 1 for a mirrored pair, unused
     int4 g[kMaxG];     // flush: cube row, crossline, window start, window length (samples)
-    int baseb[kMaxG];  // paired slots: window base of the mirrored trace
     int rowb[kMaxG];   // paired slots: cube row of the mirrored trace (-1: none)
+    float r2[kMaxG][kTX];  // r^2 of the slot's trace(s) to each consumer warp's crossline
 };
 
 struct AdjLayout {
@@ -167,7 +167,7 @@ __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
     fence_proxy_async_smem();  // the consumers' shared-memory adds -> the async proxy
     for (int k = lane; k < m.count; k += 32) {
         const int4 gg = m.g[k];  // row, crossline, ws, size
-        const uint32_t rel = static_cast<uint32_t>(m.m[k].z) + 4u * gg.z + kMagic4;
+        const uint32_t rel = static_cast<uint32_t>(m.m[k].x) + 4u * gg.z + kMagic4;
         bulk_reduce_add_f32(
             A.data + (static_cast<size_t>(gg.x) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
             smem_abs + rel, 4u * gg.w);
@@ -394,20 +394,24 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                     L.stage +
                     (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) * 4u;
                 const int slot = __popc(nzmask & ((1u << lane) - 1u));
-                const unsigned pm = __reduce_or_sync(
-                    0xffffffffu, take && size > 0 && rowb >= 0 ? (1u << slot) : 0u);
                 if (take && size > 0) {
-                    m.m[slot] = make_int4(kc, __float_as_int(dx2),
-                                          static_cast<int>(dst_rel - 4u * ws - kMagic4),
-                                          __float_as_int(static_cast<float>(ws)));
+                    m.m[slot] = make_int4(static_cast<int>(dst_rel - 4u * ws - kMagic4),
+                                          static_cast<int>(dst_rel + 4u * size - 4u * ws - kMagic4),
+                                          rowb >= 0 ? 1 : 0, 0);
                     m.g[slot] = make_int4(row, kc, ws, size);
-                    m.baseb[slot] = static_cast<int>(dst_rel + 4u * size - 4u * ws - kMagic4);
                     m.rowb[slot] = rowb;
+                    // r^2 to each consumer warp's output crossline, with the consumers'
+                    // arithmetic (trace_r2), so that each warp reads it instead
+                    float rr[kTX];
+#pragma unroll
+                    for (int w = 0; w < kTX; ++w)
+                        rr[w] = trace_r2(kc - (x0 + w + P.xoff), P.d_xl, dx2);
+                    float4* r2d = reinterpret_cast<float4*>(&m.r2[slot][0]);
+#pragma unroll
+                    for (int w = 0; w < kTX; w += 4)
+                        r2d[w / 4] = make_float4(rr[w], rr[w + 1], rr[w + 2], rr[w + 3]);
                 }
-                if (lane == 0) {
-                    m.count = n;
-                    m.pairmask = pm;
-                }
+                if (lane == 0) m.count = n;
                 __threadfence_block();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&full[stage]);
@@ -450,15 +454,14 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         const AdjMeta& m = meta[stage];
         const int cnt = m.count;
         if (cnt < 0) break;
-        const unsigned pmask = m.pairmask;
         for (int g = 0; g < cnt; ++g) {
-            const int4 md = m.m[g];
-            const float r2 = trace_r2(md.x - xv, P.d_xl, __int_as_float(md.y));
+            const float r2 = m.r2[g][warp - 1];
             if (r2 > warpmax) continue;
+            const int4 md = m.m[g];
             uint32_t base[2];
-            base[0] = static_cast<uint32_t>(md.z);
-            if ((pmask >> g) & 1u) {
-                base[1] = static_cast<uint32_t>(m.baseb[g]);
+            base[0] = static_cast<uint32_t>(md.x);
+            if (md.z) {
+                base[1] = static_cast<uint32_t>(md.y);
                 adj_visit<AMP, 2>(smem_raw, r2, base, P.ntm1m, gmax, gmin, T2, F4, BB, MK);
             } else {
                 base[1] = 0u;
