@@ -149,7 +149,10 @@ int psm_slab_geometry(const psm_geom *g, const int32_t *out_center, const psm_sl
                       psm_geom *local, int32_t *local_center);
 /* Forward migration of a cube held in host memory, streamed through the ctx in slabs of at
  * most max_device_bytes: traces and vrms [n_il][n_xl][n_t] (host) in, image
- * [n_oi][n_ox][n_t] (host) out.  For cubes larger than the GPU's memory. */
+ * [n_oi][n_ox][n_t] (host) out.  For cubes larger than the GPU's memory.  The input inlines
+ * that consecutive slabs share stay on the device; only the new ones are uploaded.
+ * Afterwards the ctx holds the last slab's geometry and no readable traces: call
+ * psm_set_geometry before using it again. */
 int psm_forward_streamed(psm_ctx *ctx, const psm_geom *g, const int32_t *out_center,
                          const float *traces, const float *vrms, float *image,
                          int64_t max_device_bytes);

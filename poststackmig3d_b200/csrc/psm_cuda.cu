@@ -1413,15 +1413,97 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
     if (rc) return c->st.fail(rc, "one output inline exceeds the device budget");
     const size_t trace = static_cast<size_t>(g->n_xl) * g->n_t;
     const size_t row = static_cast<size_t>(g->n_ox) * g->n_t;
+    // Consecutive slabs' input inlines overlap (each output inline reads about m_il + pad_il
+    // inlines either side), so the device window rolls: the inlines the next slab shares with
+    // this one stay on the device (pair cube or 16-bit words, and Vrms), moved to the front of
+    // their buffers, and only the new inlines are uploaded and prepared.  The raw traces of
+    // the kept inlines are not kept: after this call the ctx holds the last slab's geometry
+    // and no readable traces.
+    int prev_i0 = 0, prev_i1 = 0;
+    if (n > 1) {  // size the device buffers for the widest slab once, so that none regrows
+        int w = 0;
+        for (int32_t k = 1; k < n; ++k)
+            if (slabs[k].i1 - slabs[k].i0 > slabs[w].i1 - slabs[w].i0) w = k;
+        psm_geom wide;
+        std::vector<int32_t> wc(static_cast<size_t>(slabs[w].o1 - slabs[w].o0));
+        if ((rc = psm_slab_geometry(g, out_center, &slabs[w], &wide, wc.data()))) return rc;
+        if ((rc = psm_set_geometry(c, &wide, wc.data()))) return rc;
+    }
     for (int32_t k = 0; k < n; ++k) {
         const psm_slab& s = slabs[k];
         psm_geom local;
         std::vector<int32_t> lc(static_cast<size_t>(s.o1 - s.o0));
         if ((rc = psm_slab_geometry(g, out_center, &s, &local, lc.data()))) return rc;
+        // a buffer that set_geometry had to grow was reallocated (its size changed), and
+        // its contents are gone
+        const DevBuf* bufs[4] = {&c->pairs, &c->words, &c->scales, &c->vrms};
+        size_t sizes[4];
+        for (int i = 0; i < 4; ++i) sizes[i] = bufs[i]->bytes;
+        const bool had = k > 0 && c->have_traces && c->have_vrms;
         if ((rc = psm_set_geometry(c, &local, lc.data()))) return rc;
-        if ((rc = psm_set_traces(c, traces + s.i0 * trace))) return rc;
-        if ((rc = psm_set_vrms(c, vrms + s.i0 * trace))) return rc;
+        bool same_bufs = true;
+        for (int i = 0; i < 4; ++i)
+            if ((i == 0 || i == 3 || c->store != psm::kStoreF32) && bufs[i]->bytes != sizes[i])
+                same_bufs = false;
+        int keep = 0;  // inlines [s.i0, s.i0 + keep) are already on the device
+        if (had && same_bufs && s.i0 >= prev_i0 && s.i0 < prev_i1)
+            keep = std::min(prev_i1, s.i1) - s.i0;
+        if (keep == 0) {
+            if ((rc = psm_set_traces(c, traces + s.i0 * trace))) return rc;
+            if ((rc = psm_set_vrms(c, vrms + s.i0 * trace))) return rc;
+        } else {
+            cudaSetDevice(c->device);
+            const int shift = s.i0 - prev_i0;  // inlines
+            const size_t per_il_tr = static_cast<size_t>(g->n_xl);
+            // move kept inlines to the front, front to back in chunks of at most `shift`
+            // inlines so that no copy overlaps itself
+            auto move = [&](void* base, size_t il_bytes) -> cudaError_t {
+                char* b = static_cast<char*>(base);
+                for (int a = 0; shift > 0 && a < keep; a += shift) {
+                    const int ch = std::min(shift, keep - a);
+                    cudaError_t e = cudaMemcpyAsync(b + a * il_bytes, b + (a + shift) * il_bytes,
+                                                    ch * il_bytes, cudaMemcpyDeviceToDevice,
+                                                    c->stream);
+                    if (e != cudaSuccess) return e;
+                }
+                return cudaSuccess;
+            };
+            if (c->store == psm::kStoreF32) {
+                PSM_CUDA_TRY(c->st, move(c->pairs.p, per_il_tr * c->ns * sizeof(float2)));
+            } else {
+                PSM_CUDA_TRY(c->st, move(c->words.p, per_il_tr * c->ns * sizeof(uint32_t)));
+                PSM_CUDA_TRY(c->st, move(c->scales.p, per_il_tr * sizeof(float)));
+            }
+            PSM_CUDA_TRY(c->st, move(c->vrms.p, trace * sizeof(float)));
+            const int fresh = (s.i1 - s.i0) - keep;  // new inlines, after the kept ones
+            if (fresh > 0) {
+                const size_t r0 = static_cast<size_t>(keep) * per_il_tr;
+                const size_t rows = static_cast<size_t>(fresh) * per_il_tr;
+                PSM_CUDA_TRY(c->st,
+                             cudaMemcpy2DAsync(c->data.as<float>() + r0 * c->ns,
+                                               c->ns * sizeof(float),
+                                               traces + (s.i0 + keep) * trace,
+                                               g->n_t * sizeof(float), g->n_t * sizeof(float),
+                                               rows, cudaMemcpyHostToDevice, c->stream));
+                if (c->store == psm::kStoreF32)
+                    PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>() + r0 * c->ns,
+                                                    c->pairs.as<float2>() + r0 * c->ns, rows,
+                                                    c->ns, c->stream));
+                else
+                    PSM_CUDA_TRY(c->st, quantize(c->data.as<float>() + r0 * c->ns,
+                                                 c->words.as<uint32_t>() + r0 * c->ns,
+                                                 c->scales.as<float>() + r0, rows, c->ns,
+                                                 c->store, c->stream));
+                PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.as<float>() + keep * trace,
+                                                    vrms + (s.i0 + keep) * trace,
+                                                    fresh * trace * sizeof(float),
+                                                    cudaMemcpyHostToDevice, c->stream));
+            }
+            c->have_traces = c->have_vrms = true;
+        }
         if ((rc = psm_forward(c, image + s.o0 * row))) return rc;
+        prev_i0 = s.i0;
+        prev_i1 = s.i1;
     }
     return PSM_OK;
 }

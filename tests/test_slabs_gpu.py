@@ -12,11 +12,16 @@ from helpers import geometry_for, gpu_forward
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("seed,pad_il,vel", [(71, 2, "lateral"), (72, 0, "linear")])
-def test_streamed_forward_equals_resident(seed, pad_il, vel):
+@pytest.mark.parametrize("seed,pad_il,vel,precision", [(71, 2, "lateral", "f32"),
+                                                       (72, 0, "linear", "f32"),
+                                                       (73, 1, "lateral", "bf16")])
+def test_streamed_forward_equals_resident(seed, pad_il, vel, precision):
+    """Consecutive slabs keep their shared input inlines on the device (moved to the front of
+    the buffers) and upload only the new ones; 16-bit storage moves its words and scales."""
+    import dataclasses
     W = S.random_workload(seed, 24, 13, 260, vel_kind=vel, pad_il=pad_il, pad_xl=2,
                           d_il=150.0, angle=25.0)
-    g = geometry_for(W)
+    g = dataclasses.replace(geometry_for(W), precision=precision)
     whole, _, _ = gpu_forward(W, g)
     budget = int(1.1 * slab_bytes(g, min(g.n_il, 2 * (g.m_il + g.pad_il) + 1), 1))
     assert len(plan_slabs(g, budget)) > 1
