@@ -38,10 +38,38 @@ sys.path.insert(0, ROOT)
 METRIC = ("summed input samples/s (G/s) on 1 B200, mixed/batched vs plain FP32 at stated "
           "rel err")
 UNIT = "G/s"
-# Per-term limb budget of the summation on one SM per clock: 16 SFU (MUFU) ops, 128 FP32
-# lanes / ~8 FP32 ops, 32 shared-memory words / 2 samples -> 16 terms/clk/SM for each limb.
-TERMS_PER_CLK_SM = 16.0
+# Algorithmic needs of one term (an output sample and an input trace that pass the masks) on
+# the SM limbs: one load of the staged sample pair (both interpolation operands: 8 bytes in
+# fp32 storage, 4 in 16-bit storage), one rsqrt (travel time and weight; mirrored pairs share
+# it between two traces, so half), and the fp32 lane operations of t^2, s, floor, frac, the
+# interpolation and the weighted accumulate (7; 4.5 with pairs, which add the two traces'
+# samples and interpolate once).  Peak terms/s = min over limbs of (measured rate per clock
+# per SM / need per term) x SMs x SM clock; the limbs come from psm_measure_limbs.
+FP32_OPS_PER_TERM = {False: 7.0, True: 4.5}
 N_SM = 148
+
+
+def limb_roofline(limbs, sm_mhz, achieved_gterms, paired, elem_bytes):
+    """Roofline of the summation over the measured limbs: {bound, peak (Gterm/s), per-limb
+    peaks and needs}."""
+    n_sm = int(limbs.get("n_sm") or N_SM)
+    per = {
+        "lds": (limbs["lds64_bytes_per_clk_sm"], float(elem_bytes), "B"),
+        "mufu": (limbs["rsqrt_per_clk_sm"], 0.5 if paired else 1.0, "rsqrt"),
+        "fp32": (max(limbs["ffma_per_clk_sm"], limbs["ffma2_per_clk_sm"]),
+                 FP32_OPS_PER_TERM[bool(paired)], "lane-ops"),
+    }
+    peaks = {}
+    for k, (rate, need, unit) in per.items():
+        tpc = rate / need  # terms per clock per SM
+        peaks[k] = {"rate_per_clk_sm": rate, "need_per_term": need, "unit": unit,
+                    "terms_per_clk_sm": tpc,
+                    "peak_gterms": tpc * n_sm * sm_mhz * 1e6 / 1e9}
+    bound = min(peaks, key=lambda k: peaks[k]["peak_gterms"])
+    peak = peaks[bound]["peak_gterms"]
+    for k in peaks:
+        peaks[k]["frac"] = achieved_gterms / peaks[k]["peak_gterms"]
+    return bound, peak, peaks
 
 
 def parse():
@@ -62,7 +90,10 @@ def parse():
                    help="forward kernel variant (0: autotune)")
     p.add_argument("--cpu-rows", type=int, default=2,
                    help="output inlines in the bounded CPU sample")
-    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true",
+                   help="skip the CPU legs (reference kernel sample, parity rows, binaries)")
+    p.add_argument("--no-binary-baseline", action="store_true",
+                   help="skip the whole-binary config-1 timings")
     p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
                    help="trace storage in HBM (16-bit: per-trace fp32 scale, fp32 sums)")
     p.add_argument("--compensated", action="store_true",
@@ -187,44 +218,111 @@ def cpu_reference_sample(W, g, rows, threads):
     """Time the reference's own kirchhoffKernel3DWithPadding (oracle/_ref, OpenMP build, all
     host threads) on output inlines `rows`, with the buffers its driver would prepare
     (prepareInputBufferWithPadding / prepareVelocitySliceWithPadding).  Falls back to the
-    oracle port when the reference was not built.  Returns (terms, seconds, kind)."""
+    oracle port when the reference was not built.  Returns (terms, seconds, kind, rows of the
+    image)."""
     import oracle as O
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    n_il, n_xl, n_t = W.data.shape
     t0 = g.t0()
     vr = W.vrms_cube()
-    terms = 0
-    secs = 0.0
     kind = "reference" if O.ref_available() else "port"
+    cnt = O.count_rows(vr, g.out_center, 0, g.n_oi, g.n_ox, g.pad_il, g.pad_xl, g.m_il,
+                       np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il, g.d_xl,
+                       g.amp, threads=threads) if len(rows) > 8 else None
+    terms = 0
     for r in rows:
-        c = int(g.out_center[r])
-        rs, re = max(0, c - g.m_il), min(n_il, c + g.m_il + 1)
-        il0, il1 = max(0, rs - g.pad_il), min(n_il, re + g.pad_il)
-        nbx = n_xl + 2 * g.pad_xl
-        if g.pad_xl:
-            buf = np.zeros((il1 - il0, nbx, n_t), dtype=np.float32)
-            buf[:, g.pad_xl:g.pad_xl + n_xl] = W.data[il0:il1]
-            vel = np.zeros((nbx, n_t), dtype=np.float32)
-            vel[g.pad_xl:g.pad_xl + n_xl] = vr[c]
-        else:
-            buf = W.data[il0:il1]
-            vel = vr[c]
-        il_pos = np.arange(il0, il1, dtype=np.int32)
-        cnt = O.count_rows(vr, g.out_center, r, r + 1, g.n_ox, g.pad_il, g.pad_xl, g.m_il,
-                           np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il, g.d_xl,
-                           g.amp, threads=threads)
-        terms += int(cnt[0])
+        terms += int(cnt[r]) if cnt is not None else int(O.count_rows(
+            vr, g.out_center, r, r + 1, g.n_ox, g.pad_il, g.pad_xl, g.m_il,
+            np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il, g.d_xl, g.amp,
+            threads=threads)[0])
+    if kind == "reference":
+        out, secs = O.reference_rows(W.data, vr, g.out_center, rows, g.n_ox, g.pad_il,
+                                     g.pad_xl, g.m_il, g.dt_seconds, t0, g.tan2, g.d_il,
+                                     g.d_xl, g.amp, kind="omp")
+    else:
+        out = np.empty((len(rows), g.n_ox, g.n_t), dtype=np.float32)
+        secs = 0.0
+        for k, r in enumerate(rows):
+            sub = np.ascontiguousarray(g.out_center[r:r + 1])
+            t = time.perf_counter()
+            out[k] = O.migrate_volume(W.data, vr, sub, g.n_ox, g.pad_il, g.pad_xl, g.m_il,
+                                      np.float32(g.dt_seconds), t0, np.float32(g.tan2),
+                                      g.d_il, g.d_xl, g.amp, threads=threads)[0][0]
+            secs += time.perf_counter() - t
+    return terms, secs, kind, out
+
+
+def parity_block(W, g, image, rows, ref_rows, threads):
+    """Error of the GPU image on output rows `rows` against the reference's own kernel
+    (ref_rows, FP32) and against the FP64 oracle of the same operator (fed the dequantised
+    samples for 16-bit storage): relative RMS and max error over the rows, max relative to the
+    peak of the rows."""
+    import oracle as O
+
+    def err(a, b):
+        a = np.asarray(a, dtype=np.float64)
+        b = np.asarray(b, dtype=np.float64)
+        den = float(np.sqrt(np.mean(b * b))) or 1.0
+        return {"rel_rms": float(np.sqrt(np.mean((a - b) ** 2)) / den),
+                "max_rel": float(np.abs(a - b).max() / (np.abs(b).max() or 1.0))}
+
+    got = image[rows]
+    data = W.data if g.precision == "f32" else O.dequantized(W.data, g.precision)
+    sub = np.ascontiguousarray(g.out_center[rows])
+    t = time.perf_counter()
+    r32, r64, _ = O.migrate_volume(data, W.vrms_cube(), sub, g.n_ox, g.pad_il, g.pad_xl,
+                                   g.m_il, np.float32(g.dt_seconds), g.t0(),
+                                   np.float32(g.tan2), g.d_il, g.d_xl, g.amp,
+                                   O.CONTRACT | O.F64, threads, True)
+    out = {"rows": [int(r) for r in rows],
+           "vs_fp64": err(got, r64),
+           "reference_fp32_vs_fp64": err(ref_rows, r64) if ref_rows is not None else None,
+           "vs_reference": err(got, ref_rows) if ref_rows is not None else None,
+           "reference": "kirchhoffKernel3DWithPadding compiled from the reference's sources "
+                        "(oracle/_ref, OpenMP build), same rows and buffers",
+           "fp64": "FP64 oracle of the same operator (oracle/oracle.c, masks in the "
+                   "reference's FP32 arithmetic)" + (", fed the dequantised samples"
+                                                    if g.precision != "f32" else ""),
+           "oracle_s": time.perf_counter() - t}
+    return out
+
+
+def binary_baseline(threads):
+    """Whole-program wall time on config 1 (101x101x501, pad 30/30): the reference's OpenMP
+    binary (oracle/_ref/poststackmig_omp, compiled from its sources) with n_threads = all host
+    threads and with n_threads = 1 (src/main.cpp:94-97, :423-430), and this repository's
+    poststackmig binary on the same SEG-Y and config.  G/s = real-trace terms / wall."""
+    import tempfile
+
+    import oracle as O
+    from poststackmig3d_b200 import host as H
+    from poststackmig3d_b200 import synth as S
+    if not os.path.exists(O.ref_binary("omp")):
+        return None
+    W = S.workload_config1()
+    g = geometry(W)
+    terms = int(O.count_rows(W.vrms_cube(), g.out_center, 0, g.n_oi, g.n_ox, g.pad_il,
+                             g.pad_xl, g.m_il, np.float32(g.dt_seconds), g.t0(),
+                             np.float32(g.tan2), g.d_il, g.d_xl, g.amp,
+                             threads=threads).sum())
+    res = {"workload": "config1: 101x101 traces x 501 samples, pad 30/30, one SEG-Y run "
+                       "(read, migrate, write)", "terms": terms}
+    with tempfile.TemporaryDirectory() as d:
+        for key, th in (("reference_omp_all_threads", threads), ("reference_omp_1_thread", 1)):
+            cfg = S.write_run(d, W, output=f"{key}.sgy", n_threads=th)
+            t = time.perf_counter()
+            r = O.run_ref_binary(cfg, "omp", threads=th, timeout=1800)
+            wall = time.perf_counter() - t
+            if r.returncode != 0:
+                return None
+            res[key] = {"wall_s": wall, "G/s": terms / wall / 1e9, "threads": th}
+        cfg = S.write_run(d, W, output="ours.sgy")
+        H.run_binary(cfg, timeout=600)  # first run pays the module load
         t = time.perf_counter()
-        if kind == "reference":
-            O.ref_kirchhoff_inline(buf, vel, g.n_ox, il_pos, c - il0, 0,
-                                   np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il,
-                                   g.d_xl, g.amp, kind="omp")
-        else:
-            O.kirchhoff_inline(buf, vel, g.n_ox, il_pos, c - il0, 0,
-                               np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il,
-                               g.d_xl, g.amp)
-        secs += time.perf_counter() - t
-    return terms, secs, kind
+        r = H.run_binary(cfg, timeout=600)
+        wall = time.perf_counter() - t
+        if r.returncode == 0:
+            res["poststackmig_b200"] = {"wall_s": wall, "G/s": terms / wall / 1e9}
+    return res
 
 
 def sample_rows(g, k):
@@ -243,7 +341,7 @@ def run_reference(args):
     vals = []
     kind = "reference"
     for i in range(args.warmup + args.steps):
-        terms, secs, kind = cpu_reference_sample(W, g, rows, threads)
+        terms, secs, kind, _ = cpu_reference_sample(W, g, rows, threads)
         if i >= args.warmup:
             vals.append((terms, secs))
     terms = sum(v[0] for v in vals)
@@ -288,7 +386,10 @@ def run_ours(args):
     m.set_geometry(g)
     m.set_traces(W.data)
     m.set_vrms(W.vrms_cube())
-    n_terms = m.count_terms()
+    # G/s counts the terms the launch evaluates; padded output inlines that repeat an edge
+    # inline are copies (the reference migrates them again; their terms are reported apart)
+    n_terms_all = m.count_terms()
+    n_terms = m.count_terms_computed()
     stream = torch.cuda.ExternalStream(m.stream_handle())
     tuned = None
     if args.variant:
@@ -296,6 +397,9 @@ def run_ours(args):
     else:  # project autotuner: one timed launch per kernel variant, keep the fastest
         best, ms_v = m.autotune()
         tuned = {Migrator.VARIANTS[v]: round(t, 3) for v, t in ms_v.items()}
+
+    from poststackmig3d_b200.migration import measure_limbs
+    limbs = measure_limbs(local)
 
     for _ in range(max(args.warmup, 0)):
         m.forward_async()
@@ -361,9 +465,11 @@ def run_ours(args):
                "call": "psm_forward_host on pinned host buffers (traces, Vrms in; image out)"}
 
     clocks = clk.summary()
-    sm_mhz = clocks["sm_mhz"] or 1965.0
-    peak = TERMS_PER_CLK_SM * N_SM * sm_mhz * 1e6 / 1e9  # Gterm/s
+    sm_mhz = clocks["sm_mhz"] or limbs["sm_clock_mhz"]
     achieved = n_terms / (ms * 1e-3) / 1e9
+    paired = "pairs" in Migrator.VARIANTS[m.variant()]
+    bound, peak, limb_peaks = limb_roofline(limbs, sm_mhz, achieved, paired,
+                                            8 if g.precision == "f32" else 4)
     comp_bytes = (2 * g.n_il * g.n_xl * g.n_t + g.n_oi * g.n_ox * g.n_t) * 4
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -373,24 +479,34 @@ def run_ours(args):
         hbm_peak, hbm_src = 6650.0, "fallback"
     hbm_ach = comp_bytes / (ms * 1e-3) / 1e9
     roofline = {
-        "bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gterm/s",
+        "bound": bound, "achieved": achieved, "peak": peak, "unit": "Gterm/s",
         "frac": achieved / peak,
         "traffic": profile_traffic() if g.precision == "f32" and not g.compensated else None,
-        "peak_basis": f"{TERMS_PER_CLK_SM:.0f} terms/clk/SM (SFU, FP32, LDS limbs) x {N_SM} "
-                      f"SMs x median SM clock {sm_mhz:.0f} MHz under load",
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the forward "
+                          "kernel on the 201x201 crop, scaled by term count "
+                          "(profiles/fwd_kernel_config2_201.md)",
+        "peak_basis": f"measured limbs (psm_measure_limbs) x {limbs['n_sm']} SMs x median SM "
+                      f"clock {sm_mhz:.0f} MHz under load; binding limb {bound}",
+        "limbs": limb_peaks,
         "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
                 "frac": hbm_ach / hbm_peak, "peak_source": hbm_src,
                 "algorithmic_bytes_per_launch": comp_bytes},
     }
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rows = sample_rows(g, args.cpu_rows)
-        terms, secs, kind = cpu_reference_sample(W, g, rows, threads)
+        terms, secs, kind, ref_rows = cpu_reference_sample(W, g, rows, threads)
         cpu = {"value": terms / secs / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{len(rows)} central output inlines of {W.name} "
                          f"({terms} terms, {secs:.1f} s)"}
+        if kind == "reference":
+            image = m.get_image()
+            parity = parity_block(W, g, image, rows, ref_rows, threads)
+        if not args.no_binary_baseline:
+            cpu["binary"] = binary_baseline(threads)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -398,10 +514,11 @@ def run_ours(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic (seeded)",
                 "config": config_dict(W, g, {"n_terms": n_terms,
+                                             "n_terms_copied_rows": n_terms_all - n_terms,
                                              "parallelism": f"replicas x{world}",
                                              "variant": Migrator.VARIANTS[m.variant()],
                                              "autotune_ms": tuned}),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "parity": parity, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": args.steps, "clocks": clocks}
         print(json.dumps(line), flush=True)
     m.close()
@@ -559,8 +676,12 @@ def run_batch(args):
                "host_inputs": "pageable numpy arrays (the Problem arrays)"}
 
     clocks = clk.summary()
-    sm_mhz = clocks["sm_mhz"] or 1965.0
-    peak = TERMS_PER_CLK_SM * N_SM * sm_mhz * 1e6 / 1e9
+    from poststackmig3d_b200.migration import measure_limbs
+    limbs = measure_limbs(0)
+    sm_mhz = clocks["sm_mhz"] or limbs["sm_clock_mhz"]
+    bound, peak, limb_peaks = limb_roofline(limbs, sm_mhz, value,
+                                            "pairs" in Migrator.VARIANTS[b.variant()],
+                                            8 if args.storage == "f32" else 4)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -578,10 +699,11 @@ def run_batch(args):
                        "tile_order": Batch.ORDERS[b.order()], "autotune_ms": tuned,
                        "per_problem_graph_ms": ms_sep, "persistent_graph_ms": ms_pers,
                        "l2": "inputs larger than L2 (panel cube 121 MB, images 3.9 GB)"},
-            "roofline": {"bound": "issue", "achieved": value, "peak": peak, "unit": "Gterm/s",
-                         "frac": value / peak, "traffic": None,
-                         "peak_basis": f"{TERMS_PER_CLK_SM:.0f} terms/clk/SM x {N_SM} SMs x "
-                                       f"median SM clock {sm_mhz:.0f} MHz under load"},
+            "roofline": {"bound": bound, "achieved": value, "peak": peak, "unit": "Gterm/s",
+                         "frac": value / peak, "traffic": None, "limbs": limb_peaks,
+                         "peak_basis": f"measured limbs (psm_measure_limbs) x "
+                                       f"{limbs['n_sm']} SMs x median SM clock "
+                                       f"{sm_mhz:.0f} MHz under load"},
             "cpu_baseline": None, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks}
     print(json.dumps(line), flush=True)
     b.close()

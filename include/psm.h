@@ -283,7 +283,7 @@ typedef enum {
     PSM_BATCH_PER_PROBLEM = 1  /* one grid launch per problem */
 } psm_batch_mode;
 
-/* At most 192 problems (PSM_ERR_UNSUPPORTED beyond): their parameters travel as one kernel
+/* At most 184 problems (PSM_ERR_UNSUPPORTED beyond): their parameters travel as one kernel
  * argument.  Uploads every problem (the host arrays are read again by psm_batch_reload, so
  * they must stay valid while the batch lives) and builds the tile lists (psm_tile_order).
  * Images stay on the device. */
@@ -334,6 +334,27 @@ int psm_kirchhoff_inline(const float *input_buffer, size_t n_buf_il, size_t n_bu
                          float crossline_bin_size, int amp_correction);
 /* Message of the last psm_kirchhoff_inline failure on this thread. */
 const char *psm_kirchhoff_inline_error(void);
+
+/* ---- Measured throughput of the SM limbs the summation draws on (no counterpart in the
+ * reference; a measurement for the roofline).  Probe kernels run independent operations on
+ * every SM at once; each rate is operations per SM clock per SM (from clock64 spans, so it
+ * does not depend on the clock the GPU ran at), and sm_clock_mhz the clock those spans imply
+ * over the CUDA-event time.  The "slope" rates put lane l of a warp at element floor(4 l / 5),
+ * the pattern of 32 consecutive output samples on one trace (ds/dt0 = t0 / t, about 0.8). */
+typedef struct {
+    double sm_clock_mhz;
+    int32_t n_sm;
+    double rsqrt_per_clk_sm;             /* MUFU rsqrt results */
+    double ffma_per_clk_sm;              /* scalar fp32 FMAs */
+    double ffma2_per_clk_sm;             /* fp32 FMAs issued as fma.rn.f32x2 (2 per lane) */
+    double lds64_bytes_per_clk_sm;       /* 8-byte shared loads, consecutive lanes */
+    double lds64_slope_bytes_per_clk_sm; /* 8-byte shared loads, slope pattern */
+    double atom_per_clk_sm;              /* shared fp32 atomicAdd, consecutive lanes */
+    double atom_slope_per_clk_sm;        /* the same, slope pattern */
+    double red_per_clk_sm;               /* red.shared.add.f32 (no return), consecutive */
+    double red_slope_per_clk_sm;         /* the same, slope pattern */
+} psm_limbs;
+int psm_measure_limbs(int device, psm_limbs *out);
 
 /* Forward migration that allocates no device memory (this entry point has no counterpart in
  * the reference).  It is for callers that must not call cudaMalloc: applications whose device

@@ -32,10 +32,12 @@ _ref = {}
 
 
 def build(reference: Optional[str] = None) -> None:
-    """Compile liboracle.so, and the reference into _ref/ when its sources are present."""
+    """Compile liboracle.so, and the reference into _ref/ from its source tree: `reference`,
+    else the PSM_REFERENCE_SRC environment variable (skipped when neither names a tree with
+    src/)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    ref = reference or "/root/reference"
-    if os.path.isdir(os.path.join(ref, "src")):
+    ref = reference or os.environ.get("PSM_REFERENCE_SRC")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 
@@ -70,7 +72,7 @@ def lib():
             _f64p, _f32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p,
             ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
             ctypes.c_float, _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
-            ctypes.c_int, ctypes.c_int, _f64p]
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p]
         _lib = L
     return _lib
 
@@ -148,7 +150,7 @@ def count_rows(vrms, out_center, r0, r1, n_ox, pad_il, pad_xl, m_il, dt, t0, tan
 
 
 def adjoint_volume(image64, vrms, n_il, n_xl, out_center, pad_il, pad_xl, m_il, dt, t0,
-                   tan2, d_il, d_xl, amp=True, flags=CONTRACT):
+                   tan2, d_il, d_xl, amp=True, flags=CONTRACT, threads=0):
     image64 = np.ascontiguousarray(image64, dtype=np.float64)
     n_oi, n_ox, n_t = image64.shape
     out = np.zeros((n_il, n_xl, n_t), dtype=np.float64)
@@ -157,7 +159,7 @@ def adjoint_volume(image64, vrms, n_il, n_xl, out_center, pad_il, pad_xl, m_il, 
                                 n_oi, n_ox, pad_il, pad_xl, m_il, np.float32(dt),
                                 np.ascontiguousarray(t0, dtype=np.float32), np.float32(tan2),
                                 np.float32(d_il), np.float32(d_xl), int(bool(amp)), flags,
-                                out)
+                                threads, out)
     return out
 
 
@@ -173,6 +175,26 @@ def kirchhoff_inline(buf, vel, n_out_xl, il_pos, cur_il_pos, cur_xl_start, dt, t
         cur_il_pos, cur_xl_start, np.float32(dt), np.ascontiguousarray(t0, dtype=np.float32),
         np.float32(tan2), np.float32(d_il), np.float32(d_xl), int(bool(amp)), flags)
     return out, out64, n
+
+
+def dequantized(data, precision):
+    """The fp32 samples that 16-bit storage represents: per trace scale = max |d| (1 for an
+    all-zero trace), q = round-to-nearest-even(d / scale) in bf16 or fp16, d' = q * scale
+    (fp32 product).  Mirrors the device quantisation so the FP64 oracle can be fed the same
+    operator input."""
+    d = np.ascontiguousarray(data, dtype=np.float32)
+    m = np.abs(d).max(axis=-1, keepdims=True)
+    scale = np.where(m > 0, m, np.float32(1.0)).astype(np.float32)
+    x = (d / scale).astype(np.float32)
+    if precision == "bf16":
+        u = x.view(np.uint32).astype(np.uint64)
+        u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+        q = u.astype(np.uint32).view(np.float32)
+    elif precision == "f16":
+        q = x.astype(np.float16).astype(np.float32)
+    else:
+        raise ValueError(precision)
+    return (q * scale).astype(np.float32)
 
 
 # ----------------------------------------------------------------- the reference itself
@@ -220,6 +242,40 @@ def ref_kirchhoff_inline(buf, vel, n_out_xl, il_pos, cur_il_pos, cur_xl_start, d
         np.float32(dt), np.ascontiguousarray(t0, dtype=np.float32), np.float32(tan2),
         np.float32(d_il), np.float32(d_xl), int(bool(amp)))
     return out
+
+
+def reference_rows(data, vrms, out_center, rows, n_ox, pad_il, pad_xl, m_il, dt, t0, tan2,
+                   d_il, d_xl, amp=True, kind="omp"):
+    """Output rows `rows` of the whole-volume migration computed by the reference's own
+    kirchhoffKernel3DWithPadding (libref_<kind>.so), each with the buffers its driver
+    prepares: input inlines [c - m_il - pad_il, c + m_il + 1 + pad_il) clamped to the cube,
+    crosslines padded with zero traces (prepareInputBufferWithPadding,
+    src/migration_kernel.cpp:385-468), the centre inline's Vrms with v = 0 on padded
+    crosslines (prepareVelocitySliceWithPadding, :470-511).  data and vrms [n_il][n_xl][n_t].
+    Returns (image rows [len(rows)][n_ox][n_t] float32, seconds spent in the kernel)."""
+    import time
+    n_il, n_xl, n_t = data.shape
+    out = np.empty((len(rows), n_ox, n_t), dtype=np.float32)
+    secs = 0.0
+    for k, r in enumerate(rows):
+        c = int(out_center[r])
+        rs, re = max(0, c - m_il), min(n_il, c + m_il + 1)
+        il0, il1 = max(0, rs - pad_il), min(n_il, re + pad_il)
+        nbx = n_xl + 2 * pad_xl
+        if pad_xl:
+            buf = np.zeros((il1 - il0, nbx, n_t), dtype=np.float32)
+            buf[:, pad_xl:pad_xl + n_xl] = data[il0:il1]
+            vel = np.zeros((nbx, n_t), dtype=np.float32)
+            vel[pad_xl:pad_xl + n_xl] = vrms[c]
+        else:
+            buf = data[il0:il1]
+            vel = vrms[c]
+        il_pos = np.arange(il0, il1, dtype=np.int32)
+        t = time.perf_counter()
+        out[k] = ref_kirchhoff_inline(buf, vel, n_ox, il_pos, c - il0, 0, np.float32(dt), t0,
+                                      np.float32(tan2), d_il, d_xl, amp, kind=kind)
+        secs += time.perf_counter() - t
+    return out, secs
 
 
 def write_config(path: str, **kv) -> None:

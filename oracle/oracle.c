@@ -326,30 +326,41 @@ void oracle_adjoint_volume(const double *image, const float *vrms, int32_t n_il,
                            int32_t n_xl, int32_t n_t, const int32_t *out_center,
                            int32_t n_oi, int32_t n_ox, int32_t pad_il, int32_t pad_xl,
                            int32_t m_il, float dt, const float *t0, float tan2, float d_il,
-                           float d_xl, int amp, int flags, double *data_out) {
+                           float d_xl, int amp, int flags, int n_threads, double *data_out) {
     const int contract = (flags & ORACLE_CONTRACT) != 0;
     const int64_t n_buf_xl = (int64_t)n_xl + 2 * (int64_t)pad_xl;
     const float inv_dt = 1.0f / dt;
     const float inv_dxl = 1.0f / d_xl;
     memset(data_out, 0, sizeof(double) * (size_t)n_il * n_xl * n_t);
-    for (int32_t o = 0; o < n_oi; ++o) {
-        int32_t c = out_center[o];
-        int32_t il0, il1;
-        buffer_range(c, n_il, m_il, pad_il, &il0, &il1);
-        for (int64_t xb = 0; xb < n_ox && xb < n_buf_xl; ++xb) {
-            int64_t xc = xb - pad_xl;
-            if (xc < 0 || xc >= n_xl) continue; /* v = 0 there: no terms */
-            const float *vel_x = vrms + ((int64_t)c * n_xl + xc) * n_t;
-            for (int64_t t = 0; t < n_t; ++t) {
-                point_t p = point_setup(t0[t], vel_x[t], tan2, inv_dxl, xb, n_buf_xl, contract);
-                if (!p.valid) continue;
-                double m = image[((int64_t)o * n_ox + xb) * n_t + t];
-                if (m == 0.0) continue;
-                for (int32_t il = il0; il < il1; ++il) {
-                    float dx = (float)(il - c) * d_il;
-                    float dx2 = dx * dx;
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#else
+    (void)n_threads;
+#endif
+    /* One data inline il per iteration: it receives the terms of every output inline whose
+     * buffer holds it, in (o, xb, t, k) order -- the order of the serial loop nest over o, xb,
+     * t, il, k -- so the sums do not depend on the thread count. */
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int32_t il = 0; il < n_il; ++il) {
+        for (int32_t o = 0; o < n_oi; ++o) {
+            int32_t c = out_center[o];
+            int32_t il0, il1;
+            buffer_range(c, n_il, m_il, pad_il, &il0, &il1);
+            if (il < il0 || il >= il1) continue;
+            float dx = (float)(il - c) * d_il;
+            float dx2 = dx * dx;
+            double dxd = (double)(il - c) * (double)d_il;
+            for (int64_t xb = 0; xb < n_ox && xb < n_buf_xl; ++xb) {
+                int64_t xc = xb - pad_xl;
+                if (xc < 0 || xc >= n_xl) continue; /* v = 0 there: no terms */
+                const float *vel_x = vrms + ((int64_t)c * n_xl + xc) * n_t;
+                for (int64_t t = 0; t < n_t; ++t) {
+                    double m = image[((int64_t)o * n_ox + xb) * n_t + t];
+                    if (m == 0.0) continue;
+                    point_t p = point_setup(t0[t], vel_x[t], tan2, inv_dxl, xb, n_buf_xl,
+                                            contract);
+                    if (!p.valid) continue;
                     if (dx2 > p.maxd2) continue;
-                    double dxd = (double)(il - c) * (double)d_il;
                     for (int64_t k = p.xs; k < p.xe; ++k) {
                         int64_t kc = k - pad_xl;
                         if (kc < 0 || kc >= n_xl) continue;

@@ -72,7 +72,7 @@ void oracle_adjoint_volume(const double *image, const float *vrms, int32_t n_il,
                            int32_t n_xl, int32_t n_t, const int32_t *out_center,
                            int32_t n_oi, int32_t n_ox, int32_t pad_il, int32_t pad_xl,
                            int32_t m_il, float dt, const float *t0, float tan2, float d_il,
-                           float d_xl, int amp, int flags, double *data_out);
+                           float d_xl, int amp, int flags, int n_threads, double *data_out);
 
 #ifdef __cplusplus
 }

@@ -40,6 +40,21 @@ class PsmSlab(ctypes.Structure):
                 ("i1", ctypes.c_int32)]
 
 
+class PsmLimbs(ctypes.Structure):
+    """Mirror of psm_limbs (include/psm.h)."""
+    _fields_ = [("sm_clock_mhz", ctypes.c_double), ("n_sm", ctypes.c_int32),
+                ("rsqrt_per_clk_sm", ctypes.c_double), ("ffma_per_clk_sm", ctypes.c_double),
+                ("ffma2_per_clk_sm", ctypes.c_double),
+                ("lds64_bytes_per_clk_sm", ctypes.c_double),
+                ("lds64_slope_bytes_per_clk_sm", ctypes.c_double),
+                ("atom_per_clk_sm", ctypes.c_double),
+                ("atom_slope_per_clk_sm", ctypes.c_double),
+                ("red_per_clk_sm", ctypes.c_double), ("red_slope_per_clk_sm", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class PsmError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS.get(code, code)}: {msg}")
@@ -114,6 +129,7 @@ _CUDA_SYMBOLS = [
       ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _P, ctypes.c_float, ctypes.c_float,
       ctypes.c_float, ctypes.c_int]),
     ("psm_kirchhoff_inline_error", ctypes.c_char_p, []),
+    ("psm_measure_limbs", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(PsmLimbs)]),
 ]
 
 

@@ -25,9 +25,12 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SRC = [os.path.join(CSRC, "psm_cuda.cu")]
-CUDA_DEPS = CUDA_SRC + [os.path.join(CSRC, "psm_kernels.cuh"), os.path.join(CSRC, "psm_adjoint.cuh"),
-                         os.path.join(INC, "psm.h")]
+# translation units of libpsm_cuda.so, compiled in parallel and linked into one library
+CUDA_SRC = [os.path.join(CSRC, "psm_cuda.cu"), os.path.join(CSRC, "psm_limbs.cu")]
+CUDA_HDR = [os.path.join(CSRC, h) for h in ("psm_kernels.cuh", "psm_adjoint.cuh",
+                                             "psm_segy.cuh", "psm_vrms.cuh")] + \
+    [os.path.join(INC, "psm.h")]
+CUDA_DEPS = CUDA_SRC + CUDA_HDR
 # Flush-to-zero: the reference's -ffast-math build runs with FTZ/DAZ set (GCC links
 # crtfastmath), and without it every rsqrt carries a subnormal fix-up.  Divisions and square
 # roots that must round like the reference use the explicit __f*_rn intrinsics.
@@ -52,11 +55,21 @@ def _run(cmd):
 
 
 def build_cuda(force: bool = False, extra=()) -> str:
+    """Each translation unit compiles to an object under _build/ (in parallel, only when it
+    or a header changed), then nvcc links the objects into lib/libpsm_cuda.so."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB, exist_ok=True)
+    obj_dir = os.path.join(PKG, "_build", "debug" if extra else "release")
+    os.makedirs(obj_dir, exist_ok=True)
     out = os.path.join(LIB, "libpsm_cuda.so")
-    if force or extra or _stale(out, CUDA_DEPS):
-        _run([NVCC, *ARCH, *NVCC_FLAGS, "-Xcompiler", "-fPIC", "-shared", f"-I{INC}", *extra,
-              "-o", out, *CUDA_SRC])
+    objs = [os.path.join(obj_dir, os.path.basename(s)[:-3] + ".o") for s in CUDA_SRC]
+    todo = [(s, o) for s, o in zip(CUDA_SRC, objs)
+            if force or _stale(o, [s] + CUDA_HDR)]
+    with ThreadPoolExecutor(max_workers=len(CUDA_SRC)) as ex:
+        list(ex.map(lambda so: _run([NVCC, *ARCH, *NVCC_FLAGS, "-Xcompiler", "-fPIC",
+                                     f"-I{INC}", *extra, "-c", "-o", so[1], so[0]]), todo))
+    if force or todo or _stale(out, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", out, *objs])
     return out
 
 

@@ -14,8 +14,10 @@
 // window into the data cube in HBM with a TMA bulk reduction (cp.reduce.async.bulk .add.f32)
 // and waits for the reduction to have read the stage before zeroing and reusing it.  As in
 // the forward, the traces at inlines c - d and c + d of one crossline (mirrored about the
-// output inline c) have the same r^2 to every output point: they share one slot with two
-// windows, and each term's travel time, fraction and weight are computed once for both.
+// output inline c) have the same r^2 to every output point, hence the same travel times,
+// fractions and weights: every term adds the same two shares to both.  They share one slot
+// and ONE window, which the flush adds into both traces (two bulk reductions of the same
+// shared-memory window), so a pair costs the atomics of a single trace.
 #pragma once
 
 #include "psm_kernels.cuh"
@@ -31,10 +33,10 @@ struct AdjParams {
 struct AdjMeta {
     int count;         // slots in this stage, -1 = end of stream
     int pad[3];
-    int4 m[kMaxG];     // window base (smem bytes), the mirrored trace's window base (a pair's
-                       // second window follows its first), 1 for a mirrored pair, unused
+    int m[kMaxG];      // window base (smem bytes)
     int4 g[kMaxG];     // flush: cube row, crossline, window start, window length (samples)
-    int rowb[kMaxG];   // paired slots: cube row of the mirrored trace (-1: none)
+    int rowb[kMaxG];   // paired slots: cube row of the mirrored trace (-1: none), which the
+                       // flush adds the same window into
     float r2[kMaxG][kTX];  // r^2 of the slot's trace(s) to each consumer warp's crossline
 };
 
@@ -107,14 +109,13 @@ __device__ __forceinline__ void adj_window(const FwdParams& P, const TileStats& 
     *size_out = we - ws;
 }
 
-// One term of the transpose (scalar FP32) for the NT traces of a slot (a mirrored pair: the
-// same r^2): the forward's s, frac and q, then two atomic adds into each trace's window.  A
-// failing term (MASK) returns before touching memory; a passing term's lo lies in its window
-// (adj_window), with s held below n_t - 1 (smax) so that lo + 1 stays on the trace.
-template <bool AMP, bool MASK, int NT>
-__device__ __forceinline__ void adj_term(unsigned char* sbase, float r2,
-                                         const uint32_t (&base)[2], float smax,
-                                         float T2, float F4, float BB, float MK) {
+// One term of the transpose (scalar FP32) for a slot: the forward's s, frac and q, then two
+// atomic adds into the slot's window.  A failing term (MASK) returns before touching memory;
+// a passing term's lo lies in its window (adj_window), with s held below n_t - 1 (smax) so
+// that lo + 1 stays on the trace.
+template <bool AMP, bool MASK>
+__device__ __forceinline__ void adj_term(unsigned char* sbase, float r2, uint32_t base,
+                                         float smax, float T2, float F4, float BB, float MK) {
     const float t2 = __fmaf_rn(F4, r2, T2);
     const float q = rsqrtf(t2);
     const float s = fminf(t2 * q, smax);
@@ -124,20 +125,16 @@ __device__ __forceinline__ void adj_term(unsigned char* sbase, float r2,
     const float c = AMP ? MK * q : MK;
     const float c1 = c * fr;
     const float c0 = c - c1;
-    const uint32_t o = __float_as_uint(mm) << 2;
-#pragma unroll
-    for (int n = 0; n < NT; ++n) {
-        float* p = reinterpret_cast<float*>(sbase + (base[n] + o));
-        atomicAdd(p, c0);
-        atomicAdd(p + 1, c1);
-    }
+    float* p = reinterpret_cast<float*>(sbase + (base + (__float_as_uint(mm) << 2)));
+    atomicAdd(p, c0);
+    atomicAdd(p + 1, c1);
 }
 
 // One slot for one consumer warp: the groups of blocks where some lane passes, without masks
 // where every lane of the group passes.
-template <bool AMP, int NT>
-__device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2,
-                                          const uint32_t (&base)[2], float smax,
+template <bool AMP>
+__device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2, uint32_t base,
+                                          float smax,
                                           const float (&gmax)[2], const float (&gmin)[2],
                                           const float (&T2)[kJ], const float (&F4)[kJ],
                                           const float (&BB)[kJ], const float (&MK)[kJ]) {
@@ -147,27 +144,25 @@ __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2,
             if (r2 <= gmin[gr]) {
 #pragma unroll
                 for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, false, NT>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
-                                             MK[j]);
+                    adj_term<AMP, false>(sbase, r2, base, smax, T2[j], F4[j], BB[j], MK[j]);
             } else {
 #pragma unroll
                 for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, true, NT>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
-                                            MK[j]);
+                    adj_term<AMP, true>(sbase, r2, base, smax, T2[j], F4[j], BB[j], MK[j]);
             }
         }
     }
 }
 
-// Add the windows of one released stage into the data cube (one bulk reduction per window,
-// lanes in parallel; a pair's second window follows its first) and wait until they have read
-// shared memory.
+// Add the windows of one released stage into the data cube (one bulk reduction per window and
+// trace, lanes in parallel; a pair's window goes to both of its traces) and wait until they
+// have read shared memory.
 __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
                                           uint32_t smem_abs, int lane) {
     fence_proxy_async_smem();  // the consumers' shared-memory adds -> the async proxy
     for (int k = lane; k < m.count; k += 32) {
         const int4 gg = m.g[k];  // row, crossline, ws, size
-        const uint32_t rel = static_cast<uint32_t>(m.m[k].x) + 4u * gg.z + kMagic4;
+        const uint32_t rel = static_cast<uint32_t>(m.m[k]) + 4u * gg.z + kMagic4;
         bulk_reduce_add_f32(
             A.data + (static_cast<size_t>(gg.x) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
             smem_abs + rel, 4u * gg.w);
@@ -175,7 +170,7 @@ __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
         if (rb >= 0)
             bulk_reduce_add_f32(
                 A.data + (static_cast<size_t>(rb) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
-                smem_abs + rel + 4u * gg.w, 4u * gg.w);
+                smem_abs + rel, 4u * gg.w);
     }
     bulk_commit();
     bulk_wait_read_all();
@@ -302,8 +297,8 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         const int n_inl = max(job.i1 - job.i0, 0);
         // rows of the trace list: the buffer inlines, or the mirror distances d from the centre
         // inline pc (row d holds inlines pc - d and pc + d; see row_inlines)
-        int pc = -1;
-        if (P.pairable && 2 * P.ns <= P.stage_cap && n_inl > 0) {
+        int pc = -1;  // a pair needs one window (at most ns <= stage_cap samples)
+        if (P.pairable && n_inl > 0) {
             const int c = job.pos - __ldg(P.il_pos + job.i0);
             if (c >= 0 && c < n_inl) pc = c;
         }
@@ -362,7 +357,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                 row = job.i0 + a;
                 rowb = b >= 0 ? job.i0 + b : -1;
                 adj_window(P, S, xa, xb, dx2, kc, &ws, &size);
-                slot_size = rowb >= 0 ? 2 * size : size;  // a pair's windows are the same
+                slot_size = size;  // a pair shares one window
             }
             int cum = slot_size;
 #pragma unroll
@@ -378,7 +373,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
             if (n > 0) {
                 const int stage = it % kStages;
                 const uint32_t par = ((it / kStages) & 1u) ^ 1u;
-                const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
+                const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err, P.wait_us) : 0;
                 if (!__shfl_sync(0xffffffffu, ok, 0)) {
                     alive = false;
                     break;
@@ -395,9 +390,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                     (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) * 4u;
                 const int slot = __popc(nzmask & ((1u << lane) - 1u));
                 if (take && size > 0) {
-                    m.m[slot] = make_int4(static_cast<int>(dst_rel - 4u * ws - kMagic4),
-                                          static_cast<int>(dst_rel + 4u * size - 4u * ws - kMagic4),
-                                          rowb >= 0 ? 1 : 0, 0);
+                    m.m[slot] = static_cast<int>(dst_rel - 4u * ws - kMagic4);
                     m.g[slot] = make_int4(row, kc, ws, size);
                     m.rowb[slot] = rowb;
                     // r^2 to each consumer warp's output crossline, with the consumers'
@@ -423,7 +416,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
             // end-of-stream marker in the next stage, after flushing that stage's last use
             const int stage = it % kStages;
             const uint32_t par = ((it / kStages) & 1u) ^ 1u;
-            const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
+            const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err, P.wait_us) : 0;
             if (__shfl_sync(0xffffffffu, ok, 0)) {
                 if (it >= static_cast<uint32_t>(kStages)) adj_flush(A, meta[stage], smem_abs, lane);
                 if (lane == 0) {
@@ -436,7 +429,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                     const uint32_t last = it - 1;
                     const int s2 = last % kStages;
                     const uint32_t par2 = (last / kStages) & 1u;
-                    const int ok2 = lane == 0 ? mbar_wait(&empty[s2], par2, P.err) : 0;
+                    const int ok2 = lane == 0 ? mbar_wait(&empty[s2], par2, P.err, P.wait_us) : 0;
                     if (__shfl_sync(0xffffffffu, ok2, 0)) adj_flush(A, meta[s2], smem_abs, lane);
                 }
             }
@@ -450,23 +443,15 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
     while (true) {
         const int stage = it % kStages;
         const uint32_t par = (it / kStages) & 1u;
-        if (!mbar_wait(&full[stage], par, P.err)) break;
+        if (!mbar_wait(&full[stage], par, P.err, P.wait_us)) break;
         const AdjMeta& m = meta[stage];
         const int cnt = m.count;
         if (cnt < 0) break;
         for (int g = 0; g < cnt; ++g) {
             const float r2 = m.r2[g][warp - 1];
             if (r2 > warpmax) continue;
-            const int4 md = m.m[g];
-            uint32_t base[2];
-            base[0] = static_cast<uint32_t>(md.x);
-            if (md.z) {
-                base[1] = static_cast<uint32_t>(md.y);
-                adj_visit<AMP, 2>(smem_raw, r2, base, P.ntm1m, gmax, gmin, T2, F4, BB, MK);
-            } else {
-                base[1] = 0u;
-                adj_visit<AMP, 1>(smem_raw, r2, base, P.ntm1m, gmax, gmin, T2, F4, BB, MK);
-            }
+            adj_visit<AMP>(smem_raw, r2, static_cast<uint32_t>(m.m[g]), P.ntm1m, gmax, gmin, T2,
+                           F4, BB, MK);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[stage]);

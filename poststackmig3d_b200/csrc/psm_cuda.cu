@@ -2,7 +2,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -46,6 +48,19 @@ int max_inline_window(const std::vector<Job>& jobs) {
     return m;
 }
 
+// Failure injection for tests of the error paths (set from PSM_FAULT by psm_create):
+// the g_fail_alloc-th device allocation from then on fails as if the device were out of
+// memory (-1: never).
+std::atomic<int> g_fail_alloc{-1};
+
+bool alloc_fault_due() {
+    int n = g_fail_alloc.load();
+    while (n > 0) {
+        if (g_fail_alloc.compare_exchange_weak(n, n - 1)) return n == 1;
+    }
+    return false;
+}
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -58,6 +73,7 @@ struct DevBuf {
     cudaError_t ensure(size_t n) {
         if (n <= bytes && p) return cudaSuccess;
         release();
+        if (alloc_fault_due()) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, n ? n : 16);
         if (e == cudaSuccess) bytes = n;
         return e;
@@ -361,6 +377,9 @@ struct psm_ctx {
     cudaStream_t stream = nullptr;
     Status st;
     bool have_geom = false, have_traces = false, have_vrms = false;
+    // `data` holds the fp32 cube of the resident traces (false after a streamed forward,
+    // whose kept inlines live in the staged storage only, and after least-squares migration)
+    bool traces_readable = false;
     psm_geom g{};
     int ns = 0;
     int store = psm::kStoreF32;  // trace storage of the resident cube
@@ -390,9 +409,30 @@ struct psm_ctx {
     cudaStream_t d2h_stream = nullptr;
     cudaStream_t aux_stream = nullptr;
     DevBuf d_jobs_waves;
+    // limit of the kernels' mbarrier waits (us; 0: the kernels' default of 4 s) and the
+    // test-only failure injection (psm::kFault*), both read from the environment by psm_create
+    unsigned wait_us = 0;
+    int fault = 0;
 };
 
 namespace {
+
+// Error-path knobs from the environment, for tests (read at each psm_create):
+//   PSM_WAIT_LIMIT_MS   limit of every mbarrier wait in the kernels (default 4000 ms);
+//   PSM_FAULT           "stall_producer": the forward producer leaves the first stage of
+//                       each tile unfilled, so the consumers' wait runs out and the launch
+//                       returns PSM_ERR_DEVICE; "nomem:K": the K-th device allocation from
+//                       now on fails with PSM_ERR_NOMEM.
+void read_fault_env(psm_ctx* c) {
+    if (const char* w = std::getenv("PSM_WAIT_LIMIT_MS")) {
+        const long long ms = std::atoll(w);
+        if (ms > 0 && ms < 4000000) c->wait_us = static_cast<unsigned>(ms * 1000);
+    }
+    if (const char* f = std::getenv("PSM_FAULT")) {
+        if (!std::strcmp(f, "stall_producer")) c->fault = psm::kFaultStallProducer;
+        if (!std::strncmp(f, "nomem:", 6)) g_fail_alloc.store(std::atoi(f + 6));
+    }
+}
 
 FwdParams volume_params(psm_ctx* c) {
     FwdParams P{};
@@ -405,6 +445,8 @@ FwdParams volume_params(psm_ctx* c) {
     P.il_pos = c->il_pos.as<int>();
     P.t0 = c->t0.as<float>();
     P.err = c->err.as<int>();
+    P.wait_us = c->wait_us;
+    P.fault = c->fault;
     P.n_ci = c->g.n_il;
     P.n_cx = c->g.n_xl;
     P.n_t = c->g.n_t;
@@ -448,6 +490,7 @@ int psm_create(psm_ctx** out, int device) {
     psm_ctx* c = new (std::nothrow) psm_ctx();
     if (!c) return PSM_ERR_NOMEM;
     c->device = device;
+    read_fault_env(c);
     if (cudaSetDevice(device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
@@ -508,6 +551,9 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
         return c->st.fail(PSM_ERR_ARG, "out_center out of range");
     const int store = store_of(g->precision);
     const int ns = trace_stride(g->n_t);
+    // nothing of the previous geometry stays usable, whether or not the allocations below
+    // succeed
+    c->have_geom = c->have_traces = c->have_vrms = c->traces_readable = false;
     c->g = *g;
     c->ns = ns;
     c->store = store;
@@ -563,7 +609,7 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
                                         cudaMemcpyHostToDevice, c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     c->have_geom = true;
-    c->have_traces = c->have_vrms = false;
+    c->have_traces = c->have_vrms = c->traces_readable = false;
     return PSM_OK;
 }
 
@@ -582,13 +628,13 @@ int psm_set_traces(psm_ctx* c, const float* data) {
         PSM_CUDA_TRY(c->st, quantize(c->data.as<float>(), c->words.as<uint32_t>(),
                                      c->scales.as<float>(), n_tr, c->ns, c->store, c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
-    c->have_traces = true;
+    c->have_traces = c->traces_readable = true;
     return PSM_OK;
 }
 
 int psm_get_traces(psm_ctx* c, float* data) {
     if (!c || !data) return PSM_ERR_ARG;
-    if (!c->have_traces) return c->st.fail(PSM_ERR_STATE, "no traces uploaded");
+    if (!c->traces_readable) return c->st.fail(PSM_ERR_STATE, "no readable traces on the device");
     cudaSetDevice(c->device);
     const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
     PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(data, c->g.n_t * sizeof(float), c->data.p,
@@ -654,7 +700,7 @@ int psm_set_traces_segy(psm_ctx* c, const void* records, int64_t n_records, int3
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
     c->seg_n = n_records;
     c->seg_rec_bytes = rec_bytes;
-    c->have_traces = true;
+    c->have_traces = c->traces_readable = true;
     return PSM_OK;
 }
 
@@ -1070,7 +1116,7 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
     }
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
-    c->have_traces = c->have_vrms = true;
+    c->have_traces = c->have_vrms = c->traces_readable = true;
     return read_device_error(c);
 }
 
@@ -1241,7 +1287,7 @@ int psm_lsm_cg(psm_ctx* c, const float* data, float* image, int iters, double* r
     PSM_CUDA_TRY(c->st, cudaMemcpyAsync(h.data(), hist, (iters + 1) * sizeof(double),
                                         cudaMemcpyDeviceToHost, s));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
-    c->have_traces = false;  // the pair cube now holds the last residual
+    c->have_traces = c->traces_readable = false;  // the cube now holds the last residual
     if (resid)
         for (int k = 0; k <= iters; ++k) resid[k] = std::sqrt(std::max(h[k], 0.0));
     return read_device_error(c);
@@ -1500,6 +1546,7 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
                                                     cudaMemcpyHostToDevice, c->stream));
             }
             c->have_traces = c->have_vrms = true;
+            c->traces_readable = false;  // rows before `keep` hold an earlier slab's traces
         }
         if ((rc = psm_forward(c, image + s.o0 * row))) return rc;
         prev_i0 = s.i0;
@@ -1540,6 +1587,7 @@ struct psm_batch {
     int variant = PSM_FWD_DEFAULT;
     int mode = PSM_BATCH_PERSISTENT;
     int max_inl = 1, stage_cap = 0;
+    int max_ns = 0;  // longest trace stride over the problems
     int grid = 1;  // persistent CTAs
     int order = PSM_ORDER_DEPTH_FIRST;
     // tile lists [time tile 256 / 512 samples (8 / 16 blocks a lane)][order]
@@ -1559,11 +1607,21 @@ namespace {
 
 // Shared-memory attribute and persistent grid (resident CTAs on every SM) of the batch
 // kernel K; done before a stream capture, so the graph holds only the launch.
+// Stage capacity of the persistent kernel K: the batch's (48 KB stages, or one whole trace),
+// or for a kernel built for 3 CTAs per SM 32 KB stages, so that three CTAs fit an SM.
+template <class K>
+int persistent_stage_cap(const psm_batch& b) {
+    if constexpr (K::MINB > 2) return std::max(stage_cap_for(K::MINB, K::STORE), b.max_ns);
+    return b.stage_cap;
+}
+
 template <class K>
 cudaError_t prepare_persistent(K, psm_batch& b) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN,
+                                       K::PAIRS, K::MINB>;
     const size_t smem =
-        psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
+        psm::smem_layout(b.max_inl, persistent_stage_cap<K>(b), psm::store_bytes(K::STORE))
+            .total;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -1579,13 +1637,21 @@ cudaError_t prepare_persistent(K, psm_batch& b) {
 
 template <class K>
 cudaError_t launch_persistent(K, const psm_batch& b, cudaStream_t s) {
-    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
-    const size_t smem =
-        psm::smem_layout(b.max_inl, b.stage_cap, psm::store_bytes(K::STORE)).total;
+    auto* kern = psm::fwd_batch_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN,
+                                       K::PAIRS, K::MINB>;
+    const int cap = persistent_stage_cap<K>(b);
+    const size_t smem = psm::smem_layout(b.max_inl, cap, psm::store_bytes(K::STORE)).total;
     const int w = (K::J == 16 ? 2 : 0) + b.order;
+    const psm::BatchParams* params = b.params.get();
+    std::unique_ptr<psm::BatchParams> small;
+    if constexpr (K::MINB > 2) {  // every problem stages into the smaller stages
+        small = std::make_unique<psm::BatchParams>(*b.params);
+        for (size_t i = 0; i < b.probs.size(); ++i) small->p[i].stage_cap = cap;
+        params = small.get();
+    }
     kern<<<b.grid, 32 * (psm::kTX + 1), smem, s>>>(
-        *b.params, b.items[w].as<psm::BatchItem>(), b.n_items[w], b.counter.as<int>(),
-        b.ctx->err.as<int>(), b.max_inl, b.stage_cap);
+        *params, b.items[w].as<psm::BatchItem>(), b.n_items[w], b.counter.as<int>(),
+        b.ctx->err.as<int>(), b.max_inl, cap);
     return cudaGetLastError();
 }
 
@@ -1753,6 +1819,7 @@ int psm_batch_create(psm_ctx* c, const psm_problem* problems, int n, psm_batch**
         max_il = std::max(max_il, g.n_il);
         b->max_inl = std::max(b->max_inl, max_inline_window(p.jobs_all));
         b->stage_cap = std::max(b->stage_cap, stage_cap(trace_stride(g.n_t), b->store));
+        b->max_ns = std::max(b->max_ns, trace_stride(g.n_t));
     }
     if (psm::smem_layout(b->max_inl, b->stage_cap, psm::store_bytes(b->store)).total >
         kMaxDynSmem)
@@ -1817,6 +1884,8 @@ int psm_batch_create(psm_ctx* c, const psm_problem* problems, int n, psm_batch**
         P.il_pos = b->il_pos.as<int>();
         P.t0 = p.t0.as<float>();
         P.err = c->err.as<int>();
+        P.wait_us = c->wait_us;
+        P.fault = c->fault;
         P.n_ci = g.n_il;
         P.n_cx = g.n_xl;
         P.n_t = g.n_t;
@@ -2190,16 +2259,29 @@ static_assert(kNoallocT0 + sizeof(float) * kNoallocMaxT <= PSM_NOALLOC_SCRATCH_B
 __device__ __align__(256) unsigned char g_noalloc_scratch[PSM_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kNoallocMaxDevices = 64;
+// Held for the whole of a psm_forward_noalloc call: it guards the per-device addresses and
+// the host tables below, and serialises the calls of different host threads.
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_addr[kNoallocMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on the current device (looked up once per device).
+// Host-side tables of a call (about 184 KB): static, so that a caller on a thread with a
+// small stack can use the entry point; g_noalloc_mutex guards them.
+struct NoallocTables {
+    Job jobs[kNoallocMaxRows];
+    int16_t first_row_of[kNoallocMaxInl];
+    int16_t dup_dst[kNoallocMaxRows], dup_src[kNoallocMaxRows];
+    int pos[kNoallocMaxInl];
+    float t0[kNoallocMaxT];
+};
+NoallocTables g_noalloc_tables;
+
+// Device address of g_noalloc_scratch on the current device (looked up once per device;
+// the caller holds g_noalloc_mutex).
 cudaError_t noalloc_scratch(unsigned char** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_addr[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -2226,12 +2308,14 @@ extern "C" int psm_forward_noalloc(const psm_geom* g, const int32_t* out_center,
         return PSM_ERR_UNSUPPORTED;
     const int ns = trace_stride(g->n_t);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoallocTables& T = g_noalloc_tables;
 
     // jobs: one per distinct migrated inline, and the output rows that repeat it
-    // (main.cpp:258-288, migration_kernel.cpp:404-409); fixed-size host arrays, no heap
-    Job jobs[kNoallocMaxRows];
-    int16_t first_row_of[kNoallocMaxInl];
-    int16_t dup_dst[kNoallocMaxRows], dup_src[kNoallocMaxRows];
+    // (main.cpp:258-288, migration_kernel.cpp:404-409); fixed-size static tables, no heap
+    Job* jobs = T.jobs;
+    int16_t* first_row_of = T.first_row_of;
+    int16_t *dup_dst = T.dup_dst, *dup_src = T.dup_src;
     int n_jobs = 0, n_dup = 0, max_inl = 1;
     for (int i = 0; i < g->n_il; ++i) first_row_of[i] = -1;
     for (int o = 0; o < g->n_oi; ++o) {
@@ -2264,8 +2348,8 @@ extern "C" int psm_forward_noalloc(const psm_geom* g, const int32_t* out_center,
 
     unsigned char* scratch = nullptr;
     if (noalloc_scratch(&scratch) != cudaSuccess) return PSM_ERR_CUDA;
-    int pos[kNoallocMaxInl];
-    float t0[kNoallocMaxT];
+    int* pos = T.pos;
+    float* t0 = T.t0;
     for (int i = 0; i < g->n_il; ++i) pos[i] = i;
     for (int i = 0; i < g->n_t; ++i)
         t0[i] = static_cast<float>(static_cast<double>(i) * g->dt_seconds);  // main.cpp:216

@@ -41,7 +41,14 @@ constexpr int kStages = 2;      // TMA ring depth
 constexpr int kMaxG = 32;       // traces per ring stage
 static_assert(kTX % 4 == 0, "per-slot r^2 rows are stored as float4");
 constexpr int kStageCapMin = 6144;          // samples (8 B each) per ring stage, at least
-constexpr unsigned kWaitLimit = 1u << 26;   // bounded mbarrier polls
+// mbarrier waits end after FwdParams::wait_us of %globaltimer time (kDefaultWaitUs when 0),
+// or after kWaitPollCap polls, whichever comes first
+constexpr unsigned kDefaultWaitUs = 4000000u;
+constexpr unsigned kWaitPollCap = 1u << 30;
+// FwdParams::fault: test-only failure injection, 0 in normal runs.  kFaultStallProducer: the
+// producer never arrives on (and issues no copy into) the first stage of its tile, so the
+// consumers' bounded wait on it runs out and the launch reports PSM_DEV_ERR_TIMEOUT.
+constexpr int kFaultStallProducer = 1;
 
 // Trace storage in HBM: fp32 pairs (d[t], d[t+1] - d[t]) (8 B a sample), or 16-bit words
 // (q[t] | q[t+1] << 16) of bf16 / fp16 values d / scale with one fp32 scale per trace.
@@ -77,6 +84,8 @@ struct FwdParams {
     const int* il_pos;    // [n_ci] inline positions
     const float* t0;      // [n_t]
     int* err;
+    unsigned wait_us;  // limit of every mbarrier wait in microseconds (0: kDefaultWaitUs)
+    int fault;         // test-only failure injection (kFault*), 0 normally
     int n_ci, n_cx, n_t, ns;
     int n_vx;             // crosslines of a Vrms plane
     int n_ox;             // output crosslines per row
@@ -176,10 +185,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait; false (and *err set) when the limit expires.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    for (unsigned it = 0; it < kWaitLimit; ++it)
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: false (and *err set) once limit_us (0: kDefaultWaitUs) microseconds of
+// globaltimer time have passed without the phase completing (the clock is read every 64
+// polls; kWaitPollCap polls at most).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err,
+                                          unsigned limit_us) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long lim = 1000ull * (limit_us ? limit_us : kDefaultWaitUs);
+    const unsigned long long start = global_ns();
+    for (unsigned it = 1; it < kWaitPollCap; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63u) == 0 && global_ns() - start > lim) break;
+    }
     atomicOr(err, PSM_DEV_ERR_TIMEOUT);
     return false;
 }
@@ -857,6 +880,8 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             __syncwarp();
         }
         bool alive = true;
+        const uint32_t it_begin = it;       // the ring iteration of this tile's first stage
+        uint32_t stalled = 0xffffffffu;     // test-only stall: the stage left unfilled
         int f = 0;
         while (f < total && alive) {
             const int idx = f + lane;
@@ -900,11 +925,13 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             if (n > 0) {
                 const int stage = it % kStages;
                 const uint32_t par = ((it / kStages) & 1u) ^ 1u;
-                const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err) : 0;
+                const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err, P.wait_us) : 0;
                 if (!__shfl_sync(0xffffffffu, ok, 0)) {
                     alive = false;
                     break;
                 }
+                // test-only: the tile's first stage is never filled nor arrived on
+                const bool stall = (P.fault & kFaultStallProducer) && it == it_begin;
                 StageMeta& m = meta[stage];
                 const int tot = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
                 const uint32_t dst_rel =
@@ -938,10 +965,12 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                 if (lane == 0) m.count = n;
                 __threadfence_block();
                 __syncwarp();
-                if (lane == 0)
+                if (lane == 0 && !stall)
                     mbar_arrive_expect_tx(&full[stage], static_cast<uint32_t>(tot) * EB);
                 __syncwarp();
-                if (take && size > 0) {
+                if (stall) {
+                    stalled = it;
+                } else if (take && size > 0) {
                     const size_t off = (static_cast<size_t>(row) * P.n_cx + kc) * P.ns + ws;
                     const void* src = STORE == kStoreF32
                                           ? static_cast<const void*>(P.pairs + off)
@@ -966,7 +995,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             if (lane == 0) {
                 const int stage = it % kStages;
                 const uint32_t par = ((it / kStages) & 1u) ^ 1u;
-                ok = mbar_wait(&empty[stage], par, P.err);
+                ok = mbar_wait(&empty[stage], par, P.err, P.wait_us);
                 if (ok) {
                     meta[stage].count = -1;
                     __threadfence_block();
@@ -976,6 +1005,14 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             alive = __shfl_sync(0xffffffffu, ok, 0) != 0;
             ++it;
         }
+        if (!alive && lane == 0) {
+            // a wait ran out: before the CTA can exit, let the bulk copies of this tile's
+            // last fills land (earlier fills of a stage were consumed before it was refilled);
+            // each of these waits is bounded too
+            for (uint32_t i = it > it_begin + kStages ? it - kStages : it_begin; i < it; ++i)
+                if (i != stalled) mbar_wait(&full[i % kStages], (i / kStages) & 1u, P.err, P.wait_us);
+        }
+        __syncwarp();
         return alive;
     }
 
@@ -984,7 +1021,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
     while (true) {
         const int stage = it % kStages;
         const uint32_t par = (it / kStages) & 1u;
-        if (!mbar_wait(&full[stage], par, P.err)) {
+        if (!mbar_wait(&full[stage], par, P.err, P.wait_us)) {
             alive = false;
             break;
         }
@@ -1110,7 +1147,7 @@ struct BatchItem {
 
 // Parameters of every problem of a batched launch, passed by value: they live in the
 // kernel-parameter constant bank, whose loads are cached and uniform across the CTA.
-constexpr int kMaxBatchProblems = 192;
+constexpr int kMaxBatchProblems = 184;
 struct BatchParams {
     FwdParams p[kMaxBatchProblems];
 };
@@ -1120,9 +1157,11 @@ static_assert(sizeof(BatchParams) + 64 <= 32764, "kernel parameters are limited 
 // counter) until the list is exhausted, with the ring kept across tiles.  Problems (velocity
 // panels, sub-volumes) each have their own FwdParams.  max_inl and stage_cap are the largest
 // over the problems.  A device error (bounded wait expired) stops every CTA at its next tile.
+// MINB: CTAs per SM the kernel is built for (3: the grid kernels' fwd_kernel_o3 budget of 72
+// registers, with 32 KB stages from the host).
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
-          bool PAIRS = false>
-__global__ void __launch_bounds__(32 * (kTX + 1), 2)
+          bool PAIRS = false, int MINB = 2>
+__global__ void __launch_bounds__(32 * (kTX + 1), MINB)
     fwd_batch_kernel(const __grid_constant__ BatchParams B,
                      const BatchItem* __restrict__ items, int n_items, int* next,
                      const int* err, int max_inl, int stage_cap) {

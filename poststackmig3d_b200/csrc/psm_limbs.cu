@@ -1,0 +1,237 @@
+// Throughput of the SM limbs the diffraction summation and its transpose draw on, measured on
+// the device that runs them (psm_measure_limbs, include/psm.h).
+//
+// Each probe kernel runs a fixed number of independent operations per thread on every SM at
+// once (148 SMs x kCtasPerSm CTAs of kThreads threads, all resident together) and records the
+// SM-clock span of every CTA with clock64().  A rate per clock per SM is
+//     operations per SM / median CTA span (cycles),
+// which does not depend on the clock the GPU ran at; the clock itself is the span divided by
+// the CUDA-event time of the launch.  Every shared-memory index stays inside the CTA's static
+// array, and every loop has a fixed trip count.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "psm.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCtasPerSm = 4;  // 1024 threads per SM, 32 warps
+constexpr int kSmemWords = 4096 + 64;  // 16.6 KB of floats per CTA
+
+__device__ __forceinline__ void span_begin(unsigned long long* t) {
+    __syncthreads();
+    if (threadIdx.x == 0) *t = clock64();
+}
+__device__ __forceinline__ void span_end(unsigned long long t0, unsigned long long* spans) {
+    __syncthreads();
+    if (threadIdx.x == 0) spans[blockIdx.x] = clock64() - t0;
+}
+
+// 8 independent rsqrt chains per thread (MUFU.RSQ; the library builds with -ftz=true).
+__global__ void __launch_bounds__(kThreads) rsq_probe(int iters, float* sink,
+                                                      unsigned long long* spans) {
+    float x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = 1.5f + 0.01f * static_cast<float>(threadIdx.x + i);
+    __shared__ unsigned long long t0;
+    span_begin(&t0);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = rsqrtf(x[i]);
+    }
+    span_end(t0, spans);
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += x[i];
+    if (s == 12345.0f) sink[threadIdx.x] = s;
+}
+
+// 8 independent scalar FMA chains per thread.
+__global__ void __launch_bounds__(kThreads) ffma_probe(int iters, float* sink,
+                                                       unsigned long long* spans) {
+    float x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = 0.5f + 0.001f * static_cast<float>(threadIdx.x + i);
+    const float a = 0.999f, b = 0.0005f;
+    __shared__ unsigned long long t0;
+    span_begin(&t0);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = __fmaf_rn(x[i], a, b);
+    }
+    span_end(t0, spans);
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += x[i];
+    if (s == 12345.0f) sink[threadIdx.x] = s;
+}
+
+// 8 independent packed-pair FMA chains per thread (fma.rn.f32x2: two FMAs per lane).
+__global__ void __launch_bounds__(kThreads) ffma2_probe(int iters, float* sink,
+                                                        unsigned long long* spans) {
+    unsigned long long x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float v = 0.5f + 0.001f * static_cast<float>(threadIdx.x + i);
+        asm("mov.b64 %0, {%1, %2};" : "=l"(x[i]) : "f"(v), "f"(v + 0.25f));
+    }
+    unsigned long long a, b;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(a) : "f"(0.999f), "f"(0.998f));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(b) : "f"(0.0005f), "f"(0.0007f));
+    __shared__ unsigned long long t0;
+    span_begin(&t0);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) asm("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(x[i]) : "l"(a), "l"(b));
+    }
+    span_end(t0, spans);
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float lo, hi;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x[i]));
+        s += lo + hi;
+    }
+    if (s == 12345.0f) sink[threadIdx.x] = s;
+}
+
+// Lane l of a warp reads element base + idx(l) of an 8-byte array: idx(l) = l (consecutive),
+// or floor(4 l / 5) (the forward's lanes at 32 consecutive output samples map to trace
+// samples with ds/dt0 = t0 / t, about 0.8).  8 loads per iteration at distinct bases.
+template <bool SLOPE>
+__global__ void __launch_bounds__(kThreads) lds64_probe(int iters, float* sink,
+                                                        unsigned long long* spans) {
+    __shared__ float2 sm[kSmemWords / 2];
+    for (int i = threadIdx.x; i < kSmemWords / 2; i += blockDim.x)
+        sm[i] = make_float2(static_cast<float>(i), 1.0f);
+    const int lane = threadIdx.x & 31;
+    const int off = SLOPE ? (4 * lane) / 5 : lane;
+    float2 acc = make_float2(0.0f, 0.0f);
+    __shared__ unsigned long long t0;
+    span_begin(&t0);
+    for (int it = 0; it < iters; ++it) {
+        const float2* p = sm + ((it & 15) << 6) + off;  // base <= 960, + 7 * 128 + 31 < 2080
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float2 v = p[i * 128];
+            acc.x += v.x;
+            acc.y += v.y;
+        }
+    }
+    span_end(t0, spans);
+    if (acc.x == 12345.0f) sink[threadIdx.x] = acc.x + acc.y;
+}
+
+// Shared-memory f32 reductions: lane l adds to element base + idx(l) (as lds64_probe, 4-byte
+// elements), 8 per iteration at distinct bases; RED: red.shared.add.f32 (no return value),
+// else atomicAdd.
+template <bool SLOPE, bool RED>
+__global__ void __launch_bounds__(kThreads) atom_probe(int iters, float* sink,
+                                                       unsigned long long* spans) {
+    __shared__ float sm[kSmemWords];
+    for (int i = threadIdx.x; i < kSmemWords; i += blockDim.x) sm[i] = 0.0f;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int off = SLOPE ? (4 * lane) / 5 : lane;
+    const float v = 1.0f + 0.001f * static_cast<float>(lane);
+    __shared__ unsigned long long t0;
+    span_begin(&t0);
+    for (int it = 0; it < iters; ++it) {
+        // base <= 15 * 64 + 7 * 32 = 1184; + 7 * 384 + 31 < 3904 < kSmemWords
+        float* p = sm + ((it & 15) << 6) + warp * 32 + off;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (RED)
+                asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(
+                                 static_cast<unsigned>(__cvta_generic_to_shared(p + i * 384))),
+                             "f"(v)
+                             : "memory");
+            else
+                atomicAdd(p + i * 384, v);
+        }
+    }
+    span_end(t0, spans);
+    if (sm[threadIdx.x] == 12345.0f) sink[threadIdx.x] = sm[threadIdx.x];
+}
+
+// Median CTA span (cycles) and event time (ms) of one launch of kernel k.
+template <typename K>
+int time_probe(K k, int iters, int n_sm, double* cycles, double* ms) {
+    const int n_cta = n_sm * kCtasPerSm;
+    unsigned long long* spans = nullptr;
+    float* sink = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = PSM_OK;
+    if (cudaMalloc(&spans, sizeof(unsigned long long) * n_cta) != cudaSuccess ||
+        cudaMalloc(&sink, sizeof(float) * kThreads) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        rc = PSM_ERR_NOMEM;
+    } else {
+        k<<<n_cta, kThreads>>>(iters / 8, sink, spans);  // warm-up
+        cudaEventRecord(e0);
+        k<<<n_cta, kThreads>>>(iters, sink, spans);
+        cudaEventRecord(e1);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            rc = PSM_ERR_CUDA;
+        } else {
+            std::vector<unsigned long long> h(n_cta);
+            cudaMemcpy(h.data(), spans, sizeof(unsigned long long) * n_cta,
+                       cudaMemcpyDeviceToHost);
+            std::nth_element(h.begin(), h.begin() + n_cta / 2, h.end());
+            *cycles = static_cast<double>(h[n_cta / 2]);
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            *ms = t;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(spans);
+    cudaFree(sink);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int psm_measure_limbs(int device, psm_limbs* out) {
+    if (!out) return PSM_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return PSM_ERR_ARG;
+    int n_sm = 0;
+    if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return PSM_ERR_CUDA;
+    const double per_sm = static_cast<double>(kThreads) * kCtasPerSm;  // threads per SM
+    constexpr int kIters = 1 << 14;
+    double cyc = 0.0, ms = 0.0, clk_sum = 0.0;
+    int n_clk = 0;
+    int rc;
+    // rate per clock per SM of `ops` operations per thread
+    auto rate = [&](double ops) {
+        clk_sum += cyc / (ms * 1e-3) / 1e6;
+        ++n_clk;
+        return ops * per_sm / cyc;
+    };
+    if ((rc = time_probe(rsq_probe, kIters, n_sm, &cyc, &ms))) return rc;
+    out->rsqrt_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(ffma_probe, kIters, n_sm, &cyc, &ms))) return rc;
+    out->ffma_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(ffma2_probe, kIters, n_sm, &cyc, &ms))) return rc;
+    out->ffma2_per_clk_sm = rate(16.0 * kIters);
+    if ((rc = time_probe(lds64_probe<false>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->lds64_bytes_per_clk_sm = rate(64.0 * kIters);
+    if ((rc = time_probe(lds64_probe<true>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->lds64_slope_bytes_per_clk_sm = rate(64.0 * kIters);
+    if ((rc = time_probe(atom_probe<false, false>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->atom_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(atom_probe<true, false>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->atom_slope_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(atom_probe<false, true>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->red_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(atom_probe<true, true>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->red_slope_per_clk_sm = rate(8.0 * kIters);
+    out->sm_clock_mhz = clk_sum / n_clk;
+    out->n_sm = n_sm;
+    return PSM_OK;
+}

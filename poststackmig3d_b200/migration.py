@@ -211,6 +211,16 @@ def estimate_max_velocity(vrms: np.ndarray) -> float:
 # ----------------------------------------------------------------------------- operator
 
 
+def measure_limbs(device: int = 0) -> dict:
+    """Measured throughput of the SM limbs the summation draws on (psm_measure_limbs): MUFU
+    rsqrt, scalar and packed fp32 FMA, 8-byte shared loads and shared fp32 reductions, each
+    per SM clock per SM, and the SM clock the probes ran at."""
+    from ._lib import PsmLimbs
+    out = PsmLimbs()
+    check(_lib.cuda().psm_measure_limbs(device, ctypes.byref(out)))
+    return out.as_dict()
+
+
 class Migrator:
     """A cube resident on one GPU and its forward (migration) operator."""
 
@@ -243,6 +253,7 @@ class Migrator:
     def set_geometry(self, g: Geometry) -> None:
         oc = np.ascontiguousarray(g.out_center, dtype=np.int32)
         gc = g.to_c()
+        self.geom = None  # as in the library: no geometry unless this call succeeds
         check(self._L.psm_set_geometry(self._ctx, ctypes.byref(gc), oc.ctypes.data),
               self._err)
         self.geom = g
@@ -443,6 +454,14 @@ class Migrator:
         out = np.zeros(self.geom.n_oi, dtype=np.int64)
         check(self._L.psm_count_terms_rows(self._ctx, out.ctypes.data), self._err)
         return out
+
+    def count_terms_computed(self) -> int:
+        """Terms the forward launch evaluates: count_terms without the padded output inlines
+        that repeat an inline already migrated (the forward copies those rows; the reference
+        migrates them again, main.cpp:258-288)."""
+        rows = self.count_terms_rows()
+        _, first = np.unique(np.asarray(self.geom.out_center), return_index=True)
+        return int(rows[first].sum())
 
 
 class Problem:

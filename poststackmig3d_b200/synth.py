@@ -222,6 +222,34 @@ class Workload:
         return np.full(self.data.shape, np.float32(self.velocity), dtype=np.float32)
 
 
+def write_run(directory: str, W: "Workload", output: str = "out.sgy", fmt: int = 5,
+              **extra) -> str:
+    """Write workload W as the input of one poststackmig run in `directory`: the traces as a
+    SEG-Y file (labels W.il_labels / W.xl_labels, sample format fmt), a Vrms SEG-Y on the same
+    grid when W has a Vrms cube (else the constant velocity), and config.txt with the
+    reference's keys (src/config_parser.cpp; output_data = directory/output).  extra adds or
+    overrides keys (n_threads, ...).  Returns the config path."""
+    import os
+    dt_us = int(round(W.dt * 1e6))
+    inp = os.path.join(directory, "input.sgy")
+    write_segy(inp, W.data, W.il_labels, W.xl_labels, dt_us, fmt)
+    if W.vrms is not None:
+        vel = os.path.join(directory, "vrms.sgy")
+        write_segy(vel, W.vrms, W.il_labels, W.xl_labels, dt_us, 5, text="vrms")
+    else:
+        vel = repr(float(W.velocity))
+    kv = dict(input_data=inp, output_data=os.path.join(directory, output),
+              inline_step=float(W.d_il), crossline_step=float(W.d_xl), velocity=vel,
+              inline_padding=int(W.pad_il), crossline_padding=int(W.pad_xl),
+              angle_aperture=float(W.angle), amp_correction=bool(W.amp))
+    kv.update(extra)
+    cfg = os.path.join(directory, "config.txt")
+    with open(cfg, "w") as f:
+        for k, v in kv.items():
+            f.write(f"{k}={str(v).lower() if isinstance(v, bool) else v}\n")
+    return cfg
+
+
 def diffractor_cube(n_il=101, n_xl=101, n_t=501, dt=0.002, d=25.0, v=2000.0, t_apex=0.5,
                     f=25.0, noise=0.1, seed=1) -> np.ndarray:
     """One point diffractor at the cube centre: unit-peak Ricker placed on

@@ -56,20 +56,5 @@ def oracle_forward(W, g, flags=O.CONTRACT | O.AVX_ORDER, want64=False):
 
 
 def dequantized(data, precision):
-    """The fp32 samples that 16-bit storage represents: per trace scale = max |d| (1 for an
-    all-zero trace), q = round-to-nearest-even(d / scale) in bf16 or fp16, d' = q * scale
-    (fp32 product).  Mirrors the device quantisation so the FP64 oracle can be fed the same
-    operator input."""
-    d = np.ascontiguousarray(data, dtype=np.float32)
-    m = np.abs(d).max(axis=-1, keepdims=True)
-    scale = np.where(m > 0, m, np.float32(1.0)).astype(np.float32)
-    x = (d / scale).astype(np.float32)
-    if precision == "bf16":
-        u = x.view(np.uint32).astype(np.uint64)
-        u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
-        q = u.astype(np.uint32).view(np.float32)
-    elif precision == "f16":
-        q = x.astype(np.float16).astype(np.float32)
-    else:
-        raise ValueError(precision)
-    return (q * scale).astype(np.float32)
+    """The fp32 samples that 16-bit storage represents (oracle.dequantized)."""
+    return O.dequantized(data, precision)

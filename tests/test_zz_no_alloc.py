@@ -14,7 +14,7 @@ from poststackmig3d_b200 import Migrator, _lib
 from poststackmig3d_b200 import synth as S
 from poststackmig3d_b200._lib import PsmGeom
 
-from helpers import MAX_REL_TOL, REL_RMS_TOL, geometry_for, rel_err
+from helpers import geometry_for, rel_err
 
 
 def _fn():
@@ -42,6 +42,10 @@ def test_noalloc_rejects_bad_arguments_before_touching_a_device():
 
 @pytest.mark.gpu
 def test_noalloc_matches_forward_on_two_calls_in_a_row():
+    """Both entry points run the same kernel on the same tables, so the images are equal bit
+    for bit.  The cases run twice in a row (the array keeps the previous call's contents), the
+    second round under a free-memory check: once the library's kernels are loaded, a call
+    allocates no device memory."""
     import torch
 
     def pair_cube(data, ns):
@@ -54,7 +58,8 @@ def test_noalloc_matches_forward_on_two_calls_in_a_row():
     f = _fn()
     cases = [S.random_workload(41, 12, 15, 300, vel_kind="lateral", pad_il=2, pad_xl=3),
              S.random_workload(42, 9, 10, 130, vel_kind="linear", angle=50.0)]
-    for W in cases:  # the second call reuses the array the first one left behind
+    runs = []
+    for k, W in enumerate(cases):
         g = geometry_for(W)
         with Migrator(0) as m:  # the existing entry point
             m.set_geometry(g)
@@ -62,16 +67,28 @@ def test_noalloc_matches_forward_on_two_calls_in_a_row():
             m.set_vrms(W.vrms_cube())
             ref = m.forward()
         ns = (g.n_t + 7) & ~7
-        pairs = pair_cube(W.data, ns)
-        vrms = torch.from_numpy(W.vrms_cube()).cuda()
         img = torch.full((g.n_oi, g.n_ox, g.n_t), float("nan"), dtype=torch.float32,
                          device="cuda")
-        oc = np.ascontiguousarray(g.out_center, dtype=np.int32)
-        gc = g.to_c()
+        # the first case passes NULL: the regular-label centres clamp(o - pad_il)
+        oc = None if k == 0 else np.ascontiguousarray(g.out_center, dtype=np.int32)
+        runs.append((g.to_c(), oc, pair_cube(W.data, ns),
+                     torch.from_numpy(W.vrms_cube()).cuda(), img, ref))
+    torch.cuda.synchronize()
+
+    def call(gc, oc, pairs, vrms, img, ref):
+        img.fill_(float("nan"))
         torch.cuda.synchronize()
-        rc = f(ctypes.byref(gc), oc.ctypes.data, pairs.data_ptr(), vrms.data_ptr(),
-               img.data_ptr(), None)
+        rc = f(ctypes.byref(gc), None if oc is None else oc.ctypes.data, pairs.data_ptr(),
+               vrms.data_ptr(), img.data_ptr(), None)
         assert rc == 0
         got = img.cpu().numpy()
-        rms, mx = rel_err(got, ref)
-        assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (rms, mx)
+        assert np.array_equal(got, ref), rel_err(got, ref)
+
+    for r in runs:  # the first round loads the library's kernels on this device
+        call(*r)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for r in runs:  # the second call of each case reuses what the previous calls left
+        call(*r)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
