@@ -409,6 +409,11 @@ struct psm_ctx {
     cudaStream_t d2h_stream = nullptr;
     cudaStream_t aux_stream = nullptr;
     DevBuf d_jobs_waves;
+    // psm_forward_streamed: the next slab's new inlines staged during the current slab's
+    // migration (fp32 rows of ns samples, Vrms rows), two slab images in turn, and the events
+    // that order staging, placement and the image copies
+    DevBuf str_tr, str_v, str_img[2];
+    cudaEvent_t ev_placed = nullptr, ev_staged = nullptr, ev_done[2] = {nullptr, nullptr};
     // limit of the kernels' mbarrier waits (us; 0: the kernels' default of 4 s) and the
     // test-only failure injection (psm::kFault*), both read from the environment by psm_create
     unsigned wait_us = 0;
@@ -526,6 +531,9 @@ int psm_destroy(psm_ctx* c) {
     if (c->d2h_stream) cudaStreamDestroy(c->d2h_stream);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     c->d_jobs_waves.release();
+    for (DevBuf* b : {&c->str_tr, &c->str_v, &c->str_img[0], &c->str_img[1]}) b->release();
+    for (cudaEvent_t e : {c->ev_placed, c->ev_staged, c->ev_done[0], c->ev_done[1]})
+        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSM_OK;
@@ -661,10 +669,10 @@ int psm_set_traces_segy(psm_ctx* c, const void* records, int64_t n_records, int3
     }
     const int rec_bytes = psm::kSegyTraceHeader + 4 * c->g.n_t;
     cudaStream_t s = c->stream;
-    if (!c->copy_stream) {
+    if (!c->copy_stream)
         PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    if (!c->copied)
         PSM_CUDA_TRY(c->st, cudaEventCreateWithFlags(&c->copied, cudaEventDisableTiming));
-    }
     PSM_CUDA_TRY(c->st, c->seg_rec.ensure(static_cast<size_t>(n_records) * rec_bytes));
     PSM_CUDA_TRY(c->st, c->seg_pos.ensure(static_cast<size_t>(n_records) * sizeof(int32_t)));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->data.p, 0, n_tr * c->ns * sizeof(float), s));
@@ -1457,56 +1465,75 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
     int32_t n = 0;
     int rc = psm_plan_slabs(g, out_center, max_device_bytes, slabs.data(), g->n_oi, &n);
     if (rc) return c->st.fail(rc, "one output inline exceeds the device budget");
-    const size_t trace = static_cast<size_t>(g->n_xl) * g->n_t;
-    const size_t row = static_cast<size_t>(g->n_ox) * g->n_t;
+    cudaSetDevice(c->device);
+    const size_t trace = static_cast<size_t>(g->n_xl) * g->n_t;  // floats of one inline
+    const size_t row = static_cast<size_t>(g->n_ox) * g->n_t;    // floats of one output inline
+    const size_t per_il_tr = static_cast<size_t>(g->n_xl);
+    const int ns = trace_stride(g->n_t);
     // Consecutive slabs' input inlines overlap (each output inline reads about m_il + pad_il
     // inlines either side), so the device window rolls: the inlines the next slab shares with
     // this one stay on the device (pair cube or 16-bit words, and Vrms), moved to the front of
-    // their buffers, and only the new inlines are uploaded and prepared.  The raw traces of
-    // the kept inlines are not kept: after this call the ctx holds the last slab's geometry
-    // and no readable traces.
-    int prev_i0 = 0, prev_i1 = 0;
-    if (n > 1) {  // size the device buffers for the widest slab once, so that none regrows
-        int w = 0;
-        for (int32_t k = 1; k < n; ++k)
-            if (slabs[k].i1 - slabs[k].i0 > slabs[w].i1 - slabs[w].i0) w = k;
-        psm_geom wide;
-        std::vector<int32_t> wc(static_cast<size_t>(slabs[w].o1 - slabs[w].o0));
-        if ((rc = psm_slab_geometry(g, out_center, &slabs[w], &wide, wc.data()))) return rc;
-        if ((rc = psm_set_geometry(c, &wide, wc.data()))) return rc;
-    }
+    // their buffers, and only the new inlines are uploaded and prepared.  The new inlines of
+    // slab k + 1 go up into a staging area while slab k migrates, and slab k's image returns
+    // to the host while slab k + 1 migrates (two image buffers in turn), so the copies hide
+    // behind the kernels.  The raw traces of the kept inlines are not kept: after this call
+    // the ctx holds the last slab's geometry and no readable traces.
+    std::vector<psm_geom> loc(static_cast<size_t>(n));
+    std::vector<std::vector<int32_t>> lcs(static_cast<size_t>(n));
+    std::vector<int> keep(static_cast<size_t>(n), 0);  // inlines shared with the slab before
+    int wide = 0, max_oi = 0, max_fresh = 0;
     for (int32_t k = 0; k < n; ++k) {
-        const psm_slab& s = slabs[k];
-        psm_geom local;
-        std::vector<int32_t> lc(static_cast<size_t>(s.o1 - s.o0));
-        if ((rc = psm_slab_geometry(g, out_center, &s, &local, lc.data()))) return rc;
+        const psm_slab& sl = slabs[k];
+        lcs[k].resize(static_cast<size_t>(sl.o1 - sl.o0));
+        if ((rc = psm_slab_geometry(g, out_center, &sl, &loc[k], lcs[k].data()))) return rc;
+        if (sl.i1 - sl.i0 > slabs[wide].i1 - slabs[wide].i0) wide = k;
+        max_oi = std::max(max_oi, sl.o1 - sl.o0);
+        if (k > 0 && sl.i0 >= slabs[k - 1].i0 && sl.i0 < slabs[k - 1].i1)
+            keep[k] = std::min(slabs[k - 1].i1, sl.i1) - sl.i0;
+        if (k > 0 && keep[k] > 0) max_fresh = std::max(max_fresh, (sl.i1 - sl.i0) - keep[k]);
+    }
+    // size the device buffers for the widest slab once, so that none regrows
+    if (n > 1 && (rc = psm_set_geometry(c, &loc[wide], lcs[wide].data()))) return rc;
+    for (cudaStream_t* t : {&c->copy_stream, &c->d2h_stream})
+        if (!*t) PSM_CUDA_TRY(c->st, cudaStreamCreateWithFlags(t, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c->ev_placed, &c->ev_staged, &c->ev_done[0], &c->ev_done[1]})
+        if (!*e) PSM_CUDA_TRY(c->st, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    const size_t fresh_rows = static_cast<size_t>(std::max(max_fresh, 1)) * per_il_tr;
+    PSM_CUDA_TRY(c->st, c->str_tr.ensure(fresh_rows * ns * sizeof(float)));
+    PSM_CUDA_TRY(c->st, c->str_v.ensure(fresh_rows * g->n_t * sizeof(float)));
+    for (DevBuf& b : c->str_img)
+        PSM_CUDA_TRY(c->st, b.ensure(static_cast<size_t>(max_oi) * row * sizeof(float)));
+    // the staged rows' tail samples (n_t .. ns - 1) stay zero, as in the resident cube
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->str_tr.p, 0, fresh_rows * ns * sizeof(float),
+                                        c->stream));
+    bool staged = false;  // the next slab's new inlines are in the staging area
+    auto fresh_of = [&](int k) { return (slabs[k].i1 - slabs[k].i0) - keep[k]; };
+    for (int32_t k = 0; k < n; ++k) {
+        const psm_slab& sl = slabs[k];
         // a buffer that set_geometry had to grow was reallocated (its size changed), and
         // its contents are gone
         const DevBuf* bufs[4] = {&c->pairs, &c->words, &c->scales, &c->vrms};
         size_t sizes[4];
         for (int i = 0; i < 4; ++i) sizes[i] = bufs[i]->bytes;
         const bool had = k > 0 && c->have_traces && c->have_vrms;
-        if ((rc = psm_set_geometry(c, &local, lc.data()))) return rc;
+        // (waits for slab k - 1's kernel: psm_set_geometry synchronises the stream)
+        if ((rc = psm_set_geometry(c, &loc[k], lcs[k].data()))) return rc;
         bool same_bufs = true;
         for (int i = 0; i < 4; ++i)
             if ((i == 0 || i == 3 || c->store != psm::kStoreF32) && bufs[i]->bytes != sizes[i])
                 same_bufs = false;
-        int keep = 0;  // inlines [s.i0, s.i0 + keep) are already on the device
-        if (had && same_bufs && s.i0 >= prev_i0 && s.i0 < prev_i1)
-            keep = std::min(prev_i1, s.i1) - s.i0;
-        if (keep == 0) {
-            if ((rc = psm_set_traces(c, traces + s.i0 * trace))) return rc;
-            if ((rc = psm_set_vrms(c, vrms + s.i0 * trace))) return rc;
+        if (!(had && same_bufs && keep[k] > 0 && staged)) {  // the whole slab, uploaded now
+            if ((rc = psm_set_traces(c, traces + sl.i0 * trace))) return rc;
+            if ((rc = psm_set_vrms(c, vrms + sl.i0 * trace))) return rc;
         } else {
-            cudaSetDevice(c->device);
-            const int shift = s.i0 - prev_i0;  // inlines
-            const size_t per_il_tr = static_cast<size_t>(g->n_xl);
+            const int shift = sl.i0 - slabs[k - 1].i0;  // inlines
+            const int kp = keep[k];
             // move kept inlines to the front, front to back in chunks of at most `shift`
             // inlines so that no copy overlaps itself
             auto move = [&](void* base, size_t il_bytes) -> cudaError_t {
                 char* b = static_cast<char*>(base);
-                for (int a = 0; shift > 0 && a < keep; a += shift) {
-                    const int ch = std::min(shift, keep - a);
+                for (int a = 0; shift > 0 && a < kp; a += shift) {
+                    const int ch = std::min(shift, kp - a);
                     cudaError_t e = cudaMemcpyAsync(b + a * il_bytes, b + (a + shift) * il_bytes,
                                                     ch * il_bytes, cudaMemcpyDeviceToDevice,
                                                     c->stream);
@@ -1515,44 +1542,86 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
                 return cudaSuccess;
             };
             if (c->store == psm::kStoreF32) {
-                PSM_CUDA_TRY(c->st, move(c->pairs.p, per_il_tr * c->ns * sizeof(float2)));
+                PSM_CUDA_TRY(c->st, move(c->pairs.p, per_il_tr * ns * sizeof(float2)));
             } else {
-                PSM_CUDA_TRY(c->st, move(c->words.p, per_il_tr * c->ns * sizeof(uint32_t)));
+                PSM_CUDA_TRY(c->st, move(c->words.p, per_il_tr * ns * sizeof(uint32_t)));
                 PSM_CUDA_TRY(c->st, move(c->scales.p, per_il_tr * sizeof(float)));
             }
             PSM_CUDA_TRY(c->st, move(c->vrms.p, trace * sizeof(float)));
-            const int fresh = (s.i1 - s.i0) - keep;  // new inlines, after the kept ones
+            const int fresh = fresh_of(k);  // new inlines, after the kept ones, from staging
             if (fresh > 0) {
-                const size_t r0 = static_cast<size_t>(keep) * per_il_tr;
+                const size_t r0 = static_cast<size_t>(kp) * per_il_tr;
                 const size_t rows = static_cast<size_t>(fresh) * per_il_tr;
-                PSM_CUDA_TRY(c->st,
-                             cudaMemcpy2DAsync(c->data.as<float>() + r0 * c->ns,
-                                               c->ns * sizeof(float),
-                                               traces + (s.i0 + keep) * trace,
-                                               g->n_t * sizeof(float), g->n_t * sizeof(float),
-                                               rows, cudaMemcpyHostToDevice, c->stream));
+                PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->stream, c->ev_staged, 0));
                 if (c->store == psm::kStoreF32)
-                    PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>() + r0 * c->ns,
-                                                    c->pairs.as<float2>() + r0 * c->ns, rows,
-                                                    c->ns, c->stream));
+                    PSM_CUDA_TRY(c->st, build_pairs(c->str_tr.as<float>(),
+                                                    c->pairs.as<float2>() + r0 * ns, rows, ns,
+                                                    c->stream));
                 else
-                    PSM_CUDA_TRY(c->st, quantize(c->data.as<float>() + r0 * c->ns,
-                                                 c->words.as<uint32_t>() + r0 * c->ns,
-                                                 c->scales.as<float>() + r0, rows, c->ns,
-                                                 c->store, c->stream));
-                PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.as<float>() + keep * trace,
-                                                    vrms + (s.i0 + keep) * trace,
-                                                    fresh * trace * sizeof(float),
-                                                    cudaMemcpyHostToDevice, c->stream));
+                    PSM_CUDA_TRY(c->st, quantize(c->str_tr.as<float>(),
+                                                 c->words.as<uint32_t>() + r0 * ns,
+                                                 c->scales.as<float>() + r0, rows, ns, c->store,
+                                                 c->stream));
+                PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.as<float>() + kp * trace,
+                                                    c->str_v.p, fresh * trace * sizeof(float),
+                                                    cudaMemcpyDeviceToDevice, c->stream));
             }
             c->have_traces = c->have_vrms = true;
-            c->traces_readable = false;  // rows before `keep` hold an earlier slab's traces
+            c->traces_readable = false;  // the raw cube rows were not moved
         }
-        if ((rc = psm_forward(c, image + s.o0 * row))) return rc;
-        prev_i0 = s.i0;
-        prev_i1 = s.i1;
+        staged = false;
+        PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_placed, c->stream));  // staging free again
+        // migrate slab k into image buffer k % 2
+        if (k == 0) PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+        float* img = c->str_img[k & 1].as<float>();
+        FwdParams P = volume_params(c);
+        P.image = img;
+        PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
+                                       c->g.amp_correction != 0, c->variant, c->stream, c->store,
+                                       c->g.compensated != 0));
+        for (const auto& cp : c->copies)  // padded output inlines repeat an edge inline
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(img + cp.first * row, img + cp.second * row,
+                                                row * sizeof(float), cudaMemcpyDeviceToDevice,
+                                                c->stream));
+        PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_done[k & 1], c->stream));
+        // while slab k migrates: stage the next slab's new inlines (once slab k's placement
+        // has read the staging area) ...
+        if (k + 1 < n && keep[k + 1] > 0 && fresh_of(k + 1) > 0) {
+            const int kp = keep[k + 1], fresh = fresh_of(k + 1);
+            const size_t first = static_cast<size_t>(slabs[k + 1].i0 + kp);
+            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, c->ev_placed, 0));
+            PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->str_tr.p, ns * sizeof(float),
+                                                  traces + first * trace,
+                                                  g->n_t * sizeof(float), g->n_t * sizeof(float),
+                                                  static_cast<size_t>(fresh) * per_il_tr,
+                                                  cudaMemcpyHostToDevice, c->copy_stream));
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->str_v.p, vrms + first * trace,
+                                                fresh * trace * sizeof(float),
+                                                cudaMemcpyHostToDevice, c->copy_stream));
+            PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_staged, c->copy_stream));
+            staged = true;
+        } else if (k + 1 < n && keep[k + 1] > 0) {
+            staged = true;  // nothing new to stage
+        }
+        // ... and return slab k - 1's image
+        if (k > 0) {
+            const psm_slab& pv = slabs[k - 1];
+            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, c->ev_done[(k - 1) & 1], 0));
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row,
+                                                c->str_img[(k - 1) & 1].p,
+                                                (pv.o1 - pv.o0) * row * sizeof(float),
+                                                cudaMemcpyDeviceToHost, c->d2h_stream));
+            PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
+        }
     }
-    return PSM_OK;
+    if (n > 0) {
+        const psm_slab& pv = slabs[n - 1];
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row, c->str_img[(n - 1) & 1].p,
+                                            (pv.o1 - pv.o0) * row * sizeof(float),
+                                            cudaMemcpyDeviceToHost, c->stream));
+    }
+    PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->copy_stream));
+    return read_device_error(c);
 }
 
 }  // extern "C"
