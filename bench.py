@@ -86,6 +86,10 @@ def parse():
                         "one persistent launch); config5 least-squares migration; config2_io "
                         "the GPU SEG-Y codec, GPU Vrms assembly and slab streaming on config 2")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    p.add_argument("--shard", action="store_true",
+                   help="N>1: one migration split over the ranks in slabs of output inlines "
+                        "(each rank holds its slab's input inlines; strong scaling) instead "
+                        "of N replicas of the whole migration (weak scaling)")
     p.add_argument("--variant", type=int, default=0,
                    help="forward kernel variant (0: autotune)")
     p.add_argument("--cpu-rows", type=int, default=2,
@@ -382,14 +386,30 @@ def run_ours(args):
     W = workload(args.workload)
     g = dataclasses.replace(geometry(W), precision=args.storage,
                             compensated=bool(args.compensated))
+    data, vrms = W.data, W.vrms_cube()
+    gl, slab = g, None
+    if args.shard:  # this rank's slab of output inlines and the input inlines it reads
+        from poststackmig3d_b200.migration import slab_geometry, split_slabs
+        c = np.asarray(g.out_center)
+        i0 = np.maximum(0, c - g.m_il - g.pad_il)
+        i1 = np.minimum(g.n_il, c + g.m_il + 1 + g.pad_il)
+        slab = split_slabs(g, world, (i1 - i0).astype(np.float64))[rank]  # work ~ buffer
+        gl = slab_geometry(g, slab)
+        data = np.ascontiguousarray(data[slab[2]:slab[3]])
+        vrms = np.ascontiguousarray(vrms[slab[2]:slab[3]])
     m = Migrator(local)
-    m.set_geometry(g)
-    m.set_traces(W.data)
-    m.set_vrms(W.vrms_cube())
+    m.set_geometry(gl)
+    m.set_traces(data)
+    m.set_vrms(vrms)
     # G/s counts the terms the launch evaluates; padded output inlines that repeat an edge
     # inline are copies (the reference migrates them again; their terms are reported apart)
     n_terms_all = m.count_terms()
-    n_terms = m.count_terms_computed()
+    n_terms = n_terms_local = m.count_terms_computed()
+    if dist and args.shard:  # the whole migration's terms
+        t = torch.tensor([n_terms_all, n_terms], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        n_terms_all, n_terms = int(t[0].item()), int(t[1].item())
+    job_scale = 1 if args.shard else world  # replicas: every rank migrates the whole cube
     stream = torch.cuda.ExternalStream(m.stream_handle())
     tuned = None
     if args.variant:
@@ -433,13 +453,13 @@ def run_ours(args):
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_max = float(t.item())
-    value = world * n_terms / (ms_max * 1e-3) / 1e9
+    value = job_scale * n_terms / (ms_max * 1e-3) / 1e9
 
     # ---- end to end through the public API: pinned host inputs -> image on the host
     e2e = None
     if not args.no_e2e:
-        h_data = torch.from_numpy(W.data).pin_memory()
-        h_vrms = torch.from_numpy(W.vrms_cube()).pin_memory()
+        h_data = torch.from_numpy(data).pin_memory()
+        h_vrms = torch.from_numpy(vrms).pin_memory()
         h_img = torch.empty(m.image_shape(), dtype=torch.float32).pin_memory()
         e2e_steps = max(1, min(args.steps, 3))
         m.forward_host(h_data, h_vrms, h_img)  # one pipelined call: upload, migrate, download
@@ -458,7 +478,7 @@ def run_ours(args):
             t = torch.tensor([e2e_ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_ms = float(t.item())
-        e2e = {"value": world * n_terms / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+        e2e = {"value": job_scale * n_terms / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
                "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": int(h_data.numel() * 4 + h_vrms.numel() * 4),
                "d2h_bytes_per_step": int(h_img.numel() * 4),
@@ -466,7 +486,7 @@ def run_ours(args):
 
     clocks = clk.summary()
     sm_mhz = clocks["sm_mhz"] or limbs["sm_clock_mhz"]
-    achieved = n_terms / (ms * 1e-3) / 1e9
+    achieved = n_terms_local / (ms * 1e-3) / 1e9  # this GPU's launch
     paired = "pairs" in Migrator.VARIANTS[m.variant()]
     bound, peak, limb_peaks = limb_roofline(limbs, sm_mhz, achieved, paired,
                                             8 if g.precision == "f32" else 4)
@@ -511,11 +531,13 @@ def run_ours(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic (seeded)",
+                "higher_is_better": True, "scaling": "strong" if args.shard else "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                 "config": config_dict(W, g, {"n_terms": n_terms,
                                              "n_terms_copied_rows": n_terms_all - n_terms,
-                                             "parallelism": f"replicas x{world}",
+                                             "parallelism": (f"output-inline slabs x{world}"
+                                                             if args.shard else
+                                                             f"replicas x{world}"),
                                              "variant": Migrator.VARIANTS[m.variant()],
                                              "autotune_ms": tuned}),
                 "roofline": roofline, "parity": parity, "cpu_baseline": cpu, "e2e": e2e,

@@ -353,6 +353,10 @@ typedef struct {
     double atom_slope_per_clk_sm;        /* the same, slope pattern */
     double red_per_clk_sm;               /* red.shared.add.f32 (no return), consecutive */
     double red_slope_per_clk_sm;         /* the same, slope pattern */
+    double atom_u32_per_clk_sm;          /* shared 32-bit integer atomicAdd, consecutive */
+    double atom_u32_slope_per_clk_sm;    /* the same, slope pattern */
+    double atom_u64_per_clk_sm;          /* shared 64-bit integer atomicAdd, consecutive */
+    double atom_u64_slope_per_clk_sm;    /* the same, slope pattern */
 } psm_limbs;
 int psm_measure_limbs(int device, psm_limbs *out);
 

@@ -49,7 +49,11 @@ class PsmLimbs(ctypes.Structure):
                 ("lds64_slope_bytes_per_clk_sm", ctypes.c_double),
                 ("atom_per_clk_sm", ctypes.c_double),
                 ("atom_slope_per_clk_sm", ctypes.c_double),
-                ("red_per_clk_sm", ctypes.c_double), ("red_slope_per_clk_sm", ctypes.c_double)]
+                ("red_per_clk_sm", ctypes.c_double), ("red_slope_per_clk_sm", ctypes.c_double),
+                ("atom_u32_per_clk_sm", ctypes.c_double),
+                ("atom_u32_slope_per_clk_sm", ctypes.c_double),
+                ("atom_u64_per_clk_sm", ctypes.c_double),
+                ("atom_u64_slope_per_clk_sm", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -28,11 +28,13 @@ struct AdjParams {
     FwdParams F;          // geometry, tables, constants (F.pairs unused)
     const float* image;   // [n_jobs][n_ox][n_t]: image of each job (duplicate rows folded)
     float* data;          // [n_ci][n_cx][ns] accumulated in place (zero it first)
+    double* data64;       // fixed-point form: [n_ci][n_cx][ns] accumulated in FP64 instead
 };
 
 struct AdjMeta {
     int count;         // slots in this stage, -1 = end of stream
-    int pad[3];
+    int tot;           // samples of the stage's windows, which lie from the stage's start
+    int pad[2];
     int m[kMaxG];      // window base (smem bytes)
     int4 g[kMaxG];     // flush: cube row, crossline, window start, window length (samples)
     int rowb[kMaxG];   // paired slots: cube row of the mirrored trace (-1: none), which the
@@ -41,11 +43,12 @@ struct AdjMeta {
 };
 
 struct AdjLayout {
-    unsigned full, empty, meta, stats, inl_klo, inl_pre, inl_dx2, stage, total;
+    unsigned full, empty, meta, stats, mk, inl_klo, inl_pre, inl_dx2, stage, total;
 };
 
-// fp32 windows: cap counts 4-byte samples per stage
-__host__ __device__ inline AdjLayout adj_layout(int max_inl, int cap) {
+// Windows of eb-byte samples (4: fp32 sums; 8: 64-bit fixed-point sums); cap counts samples
+// per stage.
+__host__ __device__ inline AdjLayout adj_layout(int max_inl, int cap, int eb = 4) {
     AdjLayout L;
     unsigned o = 0;
     L.full = o;
@@ -56,6 +59,8 @@ __host__ __device__ inline AdjLayout adj_layout(int max_inl, int cap) {
     o += sizeof(AdjMeta) * kStages;
     L.stats = o;
     o += sizeof(TileStats) * kTX;
+    L.mk = o;  // per consumer warp: max |m K| of its samples (fixed-point scale)
+    o += 4 * kTX;
     L.inl_klo = o;
     o += 4 * max_inl;
     L.inl_pre = o;
@@ -63,12 +68,25 @@ __host__ __device__ inline AdjLayout adj_layout(int max_inl, int cap) {
     L.inl_dx2 = o;
     o += 4 * max_inl;
     L.stage = o = (o + 127) & ~127u;
-    o += 4u * cap * kStages;
+    o += static_cast<unsigned>(eb) * cap * kStages;
     L.total = o;
     return L;
 }
 
 constexpr uint32_t kMagic4 = 0x2C000000u;  // (0x4B000000 << 2) mod 2^32
+constexpr uint32_t kMagic8 = 0x58000000u;  // (0x4B000000 << 3) mod 2^32
+
+// Fixed-point sums: a tile's shares are held as integers in units of 2^-s, s = 50 - e with
+// max |m K| over the tile < 2^e, so that every share (|m K q (1 - frac)| <= |m K|, q <= 1) is
+// below 2^50 and a window sample's sum of the stage's few dozen shares stays far inside
+// 64 bits; integer adds are exact and independent of their order.
+constexpr int kFixBits = 50;
+__device__ __forceinline__ int fix_shift(float mkmax) {
+    if (!(mkmax > 0.0f)) return 0;
+    int e;
+    frexpf(mkmax, &e);  // mkmax < 2^e
+    return max(-100, min(100, kFixBits - e));
+}
 
 __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -77,6 +95,14 @@ __device__ __forceinline__ void bulk_reduce_add_f32(float* dst_global, uint32_t 
                                                     uint32_t bytes) {
     asm volatile(
         "cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f32 [%0], [%1], %2;" ::"l"(
+            dst_global),
+        "r"(src_smem), "r"(bytes)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_reduce_add_f64(double* dst_global, uint32_t src_smem,
+                                                    uint32_t bytes) {
+    asm volatile(
+        "cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;" ::"l"(
             dst_global),
         "r"(src_smem), "r"(bytes)
         : "memory");
@@ -91,11 +117,13 @@ __device__ __forceinline__ void bulk_wait_all() {
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
-// Producer: the fp32 window of trace (dx2, kc): samples [ws, we) cover lo and lo + 1 of every
-// passing term of the tile; ws and we multiples of 4 (16-byte bulk-copy granularity).
-// trace_bounds puts lo of a passing term in [lolo, lohi + 1] (the extra sample for a fast s
-// that rounds up across lohi + 1), and the consumers keep s below n_t - 1, so lo + 1 <=
-// min(lohi + 2, n_t - 1): the window covers samples up to lohi + 2, or to the row's end.
+// Producer: the window of trace (dx2, kc): samples [ws, we) cover lo and lo + 1 of every
+// passing term of the tile; ws and we multiples of A = 16 bytes / sample size (the bulk-copy
+// granularity).  trace_bounds puts lo of a passing term in [lolo, lohi + 1] (the extra sample
+// for a fast s that rounds up across lohi + 1), and the consumers keep s below n_t - 1, so
+// lo + 1 <= min(lohi + 2, n_t - 1): the window covers samples up to lohi + 2, or to the row's
+// end.
+template <int A>
 __device__ __forceinline__ void adj_window(const FwdParams& P, const TileStats& S, int xa,
                                            int xb, float dx2, int kc, int* ws_out,
                                            int* size_out) {
@@ -103,8 +131,8 @@ __device__ __forceinline__ void adj_window(const FwdParams& P, const TileStats& 
     *size_out = 0;
     int lolo, lohi;
     if (!trace_bounds(P, S, xa, xb, dx2, kc, &lolo, &lohi)) return;
-    const int ws = lolo & ~3;
-    const int we = min((lohi + 3 + 3) & ~3, P.ns);  // ns >= n_t, a multiple of 8
+    const int ws = lolo & ~(A - 1);
+    const int we = min((lohi + 2 + A) & ~(A - 1), P.ns);  // ns >= n_t, a multiple of 8
     *ws_out = ws;
     *size_out = we - ws;
 }
@@ -113,7 +141,9 @@ __device__ __forceinline__ void adj_window(const FwdParams& P, const TileStats& 
 // atomic adds into the slot's window.  A failing term (MASK) returns before touching memory;
 // a passing term's lo lies in its window (adj_window), with s held below n_t - 1 (smax) so
 // that lo + 1 stays on the trace.
-template <bool AMP, bool MASK>
+// FIX: MK is m K in units of 2^-s (exact power-of-two scaling); the shares go into the
+// window as 64-bit integers (rounded to nearest).
+template <bool AMP, bool MASK, bool FIX>
 __device__ __forceinline__ void adj_term(unsigned char* sbase, float r2, uint32_t base,
                                          float smax, float T2, float F4, float BB, float MK) {
     const float t2 = __fmaf_rn(F4, r2, T2);
@@ -125,14 +155,21 @@ __device__ __forceinline__ void adj_term(unsigned char* sbase, float r2, uint32_
     const float c = AMP ? MK * q : MK;
     const float c1 = c * fr;
     const float c0 = c - c1;
-    float* p = reinterpret_cast<float*>(sbase + (base + (__float_as_uint(mm) << 2)));
-    atomicAdd(p, c0);
-    atomicAdd(p + 1, c1);
+    if (FIX) {
+        unsigned long long* p = reinterpret_cast<unsigned long long*>(
+            sbase + (base + (__float_as_uint(mm) << 3)));
+        atomicAdd(p, static_cast<unsigned long long>(__float2ll_rn(c0)));
+        atomicAdd(p + 1, static_cast<unsigned long long>(__float2ll_rn(c1)));
+    } else {
+        float* p = reinterpret_cast<float*>(sbase + (base + (__float_as_uint(mm) << 2)));
+        atomicAdd(p, c0);
+        atomicAdd(p + 1, c1);
+    }
 }
 
 // One slot for one consumer warp: the groups of blocks where some lane passes, without masks
 // where every lane of the group passes.
-template <bool AMP>
+template <bool AMP, bool FIX>
 __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2, uint32_t base,
                                           float smax,
                                           const float (&gmax)[2], const float (&gmin)[2],
@@ -144,11 +181,13 @@ __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2, uint32
             if (r2 <= gmin[gr]) {
 #pragma unroll
                 for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, false>(sbase, r2, base, smax, T2[j], F4[j], BB[j], MK[j]);
+                    adj_term<AMP, false, FIX>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
+                                              MK[j]);
             } else {
 #pragma unroll
                 for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, true>(sbase, r2, base, smax, T2[j], F4[j], BB[j], MK[j]);
+                    adj_term<AMP, true, FIX>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
+                                             MK[j]);
             }
         }
     }
@@ -156,21 +195,45 @@ __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2, uint32
 
 // Add the windows of one released stage into the data cube (one bulk reduction per window and
 // trace, lanes in parallel; a pair's window goes to both of its traces) and wait until they
-// have read shared memory.
+// have read shared memory.  FIX: the stage's 64-bit integer sums are first turned into FP64
+// in place (times 2^-s, exact below 2^53), and the data cube accumulates in FP64.
+template <bool FIX>
 __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
-                                          uint32_t smem_abs, int lane) {
-    fence_proxy_async_smem();  // the consumers' shared-memory adds -> the async proxy
-    for (int k = lane; k < m.count; k += 32) {
-        const int4 gg = m.g[k];  // row, crossline, ws, size
-        const uint32_t rel = static_cast<uint32_t>(m.m[k]) + 4u * gg.z + kMagic4;
-        bulk_reduce_add_f32(
-            A.data + (static_cast<size_t>(gg.x) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
-            smem_abs + rel, 4u * gg.w);
-        const int rb = m.rowb[k];
-        if (rb >= 0)
+                                          unsigned char* stage, uint32_t smem_abs, int lane,
+                                          double inv_scale) {
+    if (FIX) {
+        long long* w = reinterpret_cast<long long*>(stage);
+        for (int i = lane; i < m.tot; i += 32)
+            reinterpret_cast<double*>(w)[i] = static_cast<double>(w[i]) * inv_scale;
+        __syncwarp();
+    }
+    fence_proxy_async_smem();  // the shared-memory sums -> the async proxy
+    if constexpr (FIX) {
+        for (int k = lane; k < m.count; k += 32) {
+            const int4 gg = m.g[k];  // row, crossline, ws, size
+            const uint32_t rel = static_cast<uint32_t>(m.m[k]) + 8u * gg.z + kMagic8;
+            bulk_reduce_add_f64(
+                A.data64 + (static_cast<size_t>(gg.x) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
+                smem_abs + rel, 8u * gg.w);
+            const int rb = m.rowb[k];
+            if (rb >= 0)
+                bulk_reduce_add_f64(
+                    A.data64 + (static_cast<size_t>(rb) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
+                    smem_abs + rel, 8u * gg.w);
+        }
+    } else {
+        for (int k = lane; k < m.count; k += 32) {
+            const int4 gg = m.g[k];  // row, crossline, ws, size
+            const uint32_t rel = static_cast<uint32_t>(m.m[k]) + 4u * gg.z + kMagic4;
             bulk_reduce_add_f32(
-                A.data + (static_cast<size_t>(rb) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
+                A.data + (static_cast<size_t>(gg.x) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
                 smem_abs + rel, 4u * gg.w);
+            const int rb = m.rowb[k];
+            if (rb >= 0)
+                bulk_reduce_add_f32(
+                    A.data + (static_cast<size_t>(rb) * A.F.n_cx + gg.y) * A.F.ns + gg.z,
+                    smem_abs + rel, 4u * gg.w);
+        }
     }
     bulk_commit();
     bulk_wait_read_all();
@@ -179,11 +242,16 @@ __device__ __forceinline__ void adj_flush(const AdjParams& A, const AdjMeta& m,
 
 // MINB: CTAs per SM the kernel is built for (the host gives 3-CTA launches 32 KB stages): the
 // kernel is bound by the latency of its shared-memory atomics, which more warps hide.
-template <bool AMP, int MINB = 2>
+// FIX: 64-bit fixed-point window sums and an FP64 data cube (A.data64); else fp32 atomics and
+// an fp32 data cube (A.data).
+template <bool AMP, int MINB = 2, bool FIX = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjParams A) {
+    constexpr int EB = FIX ? 8 : 4;           // bytes of a window sample
+    constexpr uint32_t MAGIC = FIX ? kMagic8 : kMagic4;
     const FwdParams& P = A.F;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const AdjLayout L = adj_layout(P.max_inl, P.stage_cap);
+    const AdjLayout L = adj_layout(P.max_inl, P.stage_cap, EB);
+    float* mkw = reinterpret_cast<float*>(smem_raw + L.mk);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + L.full);
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem_raw + L.empty);
     AdjMeta* meta = reinterpret_cast<AdjMeta*>(smem_raw + L.meta);
@@ -251,6 +319,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         bmax = warp_max(bmax);
         t0min = warp_min(t0min);
         t0max = warp_max(t0max);
+        float mkm = 0.0f;
+#pragma unroll
+        for (int j = 0; j < kJ; ++j) mkm = fmaxf(mkm, fabsf(MK[j]));
+        mkm = warp_max(mkm);
         if (lane == 0) {
             TileStats s;
             s.vmin = vmin;
@@ -260,6 +332,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
             s.t0max = t0max;
             s.any = bmax >= 0.0f;
             wstats[warp - 1] = s;
+            mkw[warp - 1] = mkm;
         }
     } else if (lane == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -269,9 +342,22 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         fence_barrier_init();
     }
     __syncthreads();
+    // fixed-point scale of the tile: shares in units of 2^-s (fix_shift)
+    int shift = 0;
+    if (FIX) {
+        float mkmax = 0.0f;
+        for (int w = 0; w < kTX; ++w) mkmax = fmaxf(mkmax, mkw[w]);
+        shift = fix_shift(mkmax);
+        if (warp > 0) {
+            const float sc = ldexpf(1.0f, shift);
+#pragma unroll
+            for (int j = 0; j < kJ; ++j) MK[j] *= sc;
+        }
+    }
 
     if (warp == 0) {
         // ---------------------------------------------------------------- producer
+        const double inv_scale = ldexp(1.0, -shift);
         TileStats S;
         S.vmin = 3.0e38f;
         S.vmax = 0.0f;
@@ -356,7 +442,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                 row_inlines(pc, n_inl, lo, &a, &b);
                 row = job.i0 + a;
                 rowb = b >= 0 ? job.i0 + b : -1;
-                adj_window(P, S, xa, xb, dx2, kc, &ws, &size);
+                adj_window<16 / EB>(P, S, xa, xb, dx2, kc, &ws, &size);
                 slot_size = size;  // a pair shares one window
             }
             int cum = slot_size;
@@ -379,18 +465,23 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                     break;
                 }
                 AdjMeta& m = meta[stage];
-                if (it >= static_cast<uint32_t>(kStages)) adj_flush(A, m, smem_abs, lane);
+                unsigned char* stage_ptr =
+                    smem_raw + L.stage + static_cast<uint32_t>(EB) * stage * P.stage_cap;
+                if (it >= static_cast<uint32_t>(kStages))
+                    adj_flush<FIX>(A, m, stage_ptr, smem_abs, lane, inv_scale);
                 const int tot = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
-                // zero the accumulator region of the new windows (16 B per lane per step)
-                float4* z = reinterpret_cast<float4*>(smem_raw + L.stage +
-                                                      4u * stage * P.stage_cap);
-                for (int k = lane; k < tot / 4; k += 32) z[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                // zero the accumulator region of the new windows (16 B per lane per step;
+                // windows are 16-byte multiples)
+                float4* z = reinterpret_cast<float4*>(stage_ptr);
+                for (int k = lane; k < tot * EB / 16; k += 32)
+                    z[k] = make_float4(0.f, 0.f, 0.f, 0.f);
                 const uint32_t dst_rel =
-                    L.stage +
-                    (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) * 4u;
+                    L.stage + (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) *
+                                  static_cast<uint32_t>(EB);
                 const int slot = __popc(nzmask & ((1u << lane) - 1u));
+                if (lane == 0) m.tot = tot;
                 if (take && size > 0) {
-                    m.m[slot] = static_cast<int>(dst_rel - 4u * ws - kMagic4);
+                    m.m[slot] = static_cast<int>(dst_rel - static_cast<uint32_t>(EB) * ws - MAGIC);
                     m.g[slot] = make_int4(row, kc, ws, size);
                     m.rowb[slot] = rowb;
                     // r^2 to each consumer warp's output crossline, with the consumers'
@@ -418,7 +509,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
             const uint32_t par = ((it / kStages) & 1u) ^ 1u;
             const int ok = lane == 0 ? mbar_wait(&empty[stage], par, P.err, P.wait_us) : 0;
             if (__shfl_sync(0xffffffffu, ok, 0)) {
-                if (it >= static_cast<uint32_t>(kStages)) adj_flush(A, meta[stage], smem_abs, lane);
+                if (it >= static_cast<uint32_t>(kStages))
+                    adj_flush<FIX>(A, meta[stage],
+                                   smem_raw + L.stage + static_cast<uint32_t>(EB) * stage * P.stage_cap,
+                                   smem_abs, lane, inv_scale);
                 if (lane == 0) {
                     meta[stage].count = -1;
                     __threadfence_block();
@@ -430,7 +524,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                     const int s2 = last % kStages;
                     const uint32_t par2 = (last / kStages) & 1u;
                     const int ok2 = lane == 0 ? mbar_wait(&empty[s2], par2, P.err, P.wait_us) : 0;
-                    if (__shfl_sync(0xffffffffu, ok2, 0)) adj_flush(A, meta[s2], smem_abs, lane);
+                    if (__shfl_sync(0xffffffffu, ok2, 0))
+                        adj_flush<FIX>(A, meta[s2],
+                                       smem_raw + L.stage + static_cast<uint32_t>(EB) * s2 * P.stage_cap,
+                                       smem_abs, lane, inv_scale);
                 }
             }
         }
@@ -450,13 +547,21 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         for (int g = 0; g < cnt; ++g) {
             const float r2 = m.r2[g][warp - 1];
             if (r2 > warpmax) continue;
-            adj_visit<AMP>(smem_raw, r2, static_cast<uint32_t>(m.m[g]), P.ntm1m, gmax, gmin, T2,
-                           F4, BB, MK);
+            adj_visit<AMP, FIX>(smem_raw, r2, static_cast<uint32_t>(m.m[g]), P.ntm1m, gmax, gmin,
+                                T2, F4, BB, MK);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[stage]);
         ++it;
     }
+}
+
+// out[i] = float(in[i]) (the FP64 data cube of the fixed-point adjoint to the fp32 vector).
+__global__ void f64_to_f32_kernel(const double* __restrict__ in, float* __restrict__ out,
+                                  size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<float>(in[i]);
 }
 
 // Sum the image rows that repeat one migrated inline (the transpose of the forward's row

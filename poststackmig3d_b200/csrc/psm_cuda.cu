@@ -414,6 +414,9 @@ struct psm_ctx {
     // that order staging, placement and the image copies
     DevBuf str_tr, str_v, str_img[2];
     cudaEvent_t ev_placed = nullptr, ev_staged = nullptr, ev_done[2] = {nullptr, nullptr};
+    // adjoint: 64-bit fixed-point window sums and an FP64 data cube (else fp32 atomics)
+    bool adj_fixed = true;
+    DevBuf adj64;
     // limit of the kernels' mbarrier waits (us; 0: the kernels' default of 4 s) and the
     // test-only failure injection (psm::kFault*), both read from the environment by psm_create
     unsigned wait_us = 0;
@@ -433,6 +436,8 @@ void read_fault_env(psm_ctx* c) {
         const long long ms = std::atoll(w);
         if (ms > 0 && ms < 4000000) c->wait_us = static_cast<unsigned>(ms * 1000);
     }
+    if (const char* a = std::getenv("PSM_ADJ_ACCUM"))  // "f32": fp32 atomics in the adjoint
+        c->adj_fixed = std::strcmp(a, "f32") != 0;
     if (const char* f = std::getenv("PSM_FAULT")) {
         if (!std::strcmp(f, "stall_producer")) c->fault = psm::kFaultStallProducer;
         if (!std::strncmp(f, "nomem:", 6)) g_fail_alloc.store(std::atoi(f + 6));
@@ -531,7 +536,8 @@ int psm_destroy(psm_ctx* c) {
     if (c->d2h_stream) cudaStreamDestroy(c->d2h_stream);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     c->d_jobs_waves.release();
-    for (DevBuf* b : {&c->str_tr, &c->str_v, &c->str_img[0], &c->str_img[1]}) b->release();
+    for (DevBuf* b : {&c->str_tr, &c->str_v, &c->str_img[0], &c->str_img[1], &c->adj64})
+        b->release();
     for (cudaEvent_t e : {c->ev_placed, c->ev_staged, c->ev_done[0], c->ev_done[1]})
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1134,20 +1140,20 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
 
 namespace {
 
-constexpr int kAdjStageCapMin = 12288;  // fp32 samples per adjoint ring stage (48 KB)
-constexpr int kAdjStageCapO3 = 8192;    // the same for 3 CTAs per SM (32 KB)
-inline int adj_stage_cap(int ns, int minb = 2) {
-    return std::max(minb == 3 ? kAdjStageCapO3 : kAdjStageCapMin, ns);
+// Samples per adjoint ring stage: 48 KB stages (32 KB for 3 CTAs per SM) of 4-byte fp32 sums
+// or 8-byte fixed-point sums, and at least one whole trace.
+inline int adj_stage_cap(int ns, int minb, int eb) {
+    return std::max((minb == 3 ? 32768 : 49152) / eb, ns);
 }
 
-template <bool AMP, int MINB>
+template <bool AMP, int MINB, bool FIX>
 cudaError_t launch_adj(const psm::AdjParams& A, dim3 grid, dim3 block, size_t smem,
                        cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(psm::adj_kernel<AMP, MINB>,
+    cudaError_t e = cudaFuncSetAttribute(psm::adj_kernel<AMP, MINB, FIX>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    psm::adj_kernel<AMP, MINB><<<grid, block, smem, s>>>(A);
+    psm::adj_kernel<AMP, MINB, FIX><<<grid, block, smem, s>>>(A);
     return cudaGetLastError();
 }
 
@@ -1169,18 +1175,27 @@ int adjoint_dev(psm_ctx* c, const float* d_rows, float* d_out) {
         PSM_CUDA_TRY(c->st, cudaGetLastError());
         job_img = c->fold.as<float>();
     }
-    PSM_CUDA_TRY(c->st, cudaMemsetAsync(d_out, 0, n_tr * c->ns * sizeof(float), c->stream));
+    const bool fix = c->adj_fixed;
+    const size_t n_data = n_tr * c->ns;
     psm::AdjParams A{};
     A.F = volume_params(c);
     A.image = job_img;
     A.data = d_out;
+    if (fix) {  // FP64 data cube, converted to d_out afterwards
+        PSM_CUDA_TRY(c->st, c->adj64.ensure(n_data * sizeof(double)));
+        PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->adj64.p, 0, n_data * sizeof(double), c->stream));
+        A.data64 = c->adj64.as<double>();
+    } else {
+        PSM_CUDA_TRY(c->st, cudaMemsetAsync(d_out, 0, n_data * sizeof(float), c->stream));
+    }
+    const int eb = fix ? 8 : 4;
     // 3 CTAs per SM when their 32 KB stages (and the inline tables) fit a third of the SM
-    A.F.stage_cap = adj_stage_cap(c->ns, 3);
-    size_t smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap).total;
+    A.F.stage_cap = adj_stage_cap(c->ns, 3, eb);
+    size_t smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap, eb).total;
     const bool o3 = smem <= 75 * 1024;
     if (!o3) {
-        A.F.stage_cap = adj_stage_cap(c->ns);
-        smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap).total;
+        A.F.stage_cap = adj_stage_cap(c->ns, 2, eb);
+        smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap, eb).total;
     }
     if (smem > kMaxDynSmem)
         return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t / aperture too large for the adjoint ring");
@@ -1188,10 +1203,23 @@ int adjoint_dev(psm_ctx* c, const float* d_rows, float* d_out) {
               n_jobs);
     dim3 block(32 * (psm::kTX + 1));
     const bool amp = c->g.amp_correction != 0;
-    PSM_CUDA_TRY(c->st, o3 ? (amp ? launch_adj<true, 3>(A, grid, block, smem, c->stream)
-                                  : launch_adj<false, 3>(A, grid, block, smem, c->stream))
-                           : (amp ? launch_adj<true, 2>(A, grid, block, smem, c->stream)
-                                  : launch_adj<false, 2>(A, grid, block, smem, c->stream)));
+    cudaError_t e;
+    if (fix)
+        e = o3 ? (amp ? launch_adj<true, 3, true>(A, grid, block, smem, c->stream)
+                      : launch_adj<false, 3, true>(A, grid, block, smem, c->stream))
+               : (amp ? launch_adj<true, 2, true>(A, grid, block, smem, c->stream)
+                      : launch_adj<false, 2, true>(A, grid, block, smem, c->stream));
+    else
+        e = o3 ? (amp ? launch_adj<true, 3, false>(A, grid, block, smem, c->stream)
+                      : launch_adj<false, 3, false>(A, grid, block, smem, c->stream))
+               : (amp ? launch_adj<true, 2, false>(A, grid, block, smem, c->stream)
+                      : launch_adj<false, 2, false>(A, grid, block, smem, c->stream));
+    PSM_CUDA_TRY(c->st, e);
+    if (fix) {
+        psm::f64_to_f32_kernel<<<grid_for(n_data), 256, 0, c->stream>>>(c->adj64.as<double>(),
+                                                                         d_out, n_data);
+        PSM_CUDA_TRY(c->st, cudaGetLastError());
+    }
     return PSM_OK;
 }
 

@@ -157,6 +157,29 @@ __global__ void __launch_bounds__(kThreads) atom_probe(int iters, float* sink,
     if (sm[threadIdx.x] == 12345.0f) sink[threadIdx.x] = sm[threadIdx.x];
 }
 
+// Shared-memory integer reductions (atomicAdd on 32- or 64-bit unsigned integers, return value
+// unused), the same address patterns as atom_probe.
+template <bool SLOPE, typename T>
+__global__ void __launch_bounds__(kThreads) iatom_probe(int iters, float* sink,
+                                                        unsigned long long* spans) {
+    __shared__ T sm[kSmemWords];  // 16.6 KB (u32) or 33 KB (u64)
+    for (int i = threadIdx.x; i < kSmemWords; i += blockDim.x) sm[i] = 0;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int off = SLOPE ? (4 * lane) / 5 : lane;
+    const T v = static_cast<T>(1 + lane);
+    __shared__ unsigned long long t0;
+    span_begin(&t0);
+    for (int it = 0; it < iters; ++it) {
+        // as atom_probe: every index stays below 3904 < kSmemWords
+        T* p = sm + ((it & 15) << 6) + warp * 32 + off;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) atomicAdd(p + i * 384, v);
+    }
+    span_end(t0, spans);
+    if (sm[threadIdx.x] == static_cast<T>(12345)) sink[threadIdx.x] = 1.0f;
+}
+
 // Median CTA span (cycles) and event time (ms) of one launch of kernel k.
 template <typename K>
 int time_probe(K k, int iters, int n_sm, double* cycles, double* ms) {
@@ -231,6 +254,16 @@ extern "C" int psm_measure_limbs(int device, psm_limbs* out) {
     out->red_per_clk_sm = rate(8.0 * kIters);
     if ((rc = time_probe(atom_probe<true, true>, kIters, n_sm, &cyc, &ms))) return rc;
     out->red_slope_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(iatom_probe<false, unsigned>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->atom_u32_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(iatom_probe<true, unsigned>, kIters, n_sm, &cyc, &ms))) return rc;
+    out->atom_u32_slope_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(iatom_probe<false, unsigned long long>, kIters, n_sm, &cyc, &ms)))
+        return rc;
+    out->atom_u64_per_clk_sm = rate(8.0 * kIters);
+    if ((rc = time_probe(iatom_probe<true, unsigned long long>, kIters, n_sm, &cyc, &ms)))
+        return rc;
+    out->atom_u64_slope_per_clk_sm = rate(8.0 * kIters);
     out->sm_clock_mhz = clk_sum / n_clk;
     out->n_sm = n_sm;
     return PSM_OK;

@@ -47,8 +47,16 @@ def test_dot_product(case):
     assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs)), (lhs, rhs)
 
 
+@pytest.mark.parametrize("accum", ["fixed", "f32"])
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"seed{c['seed']}")
-def test_adjoint_matches_oracle(case):
+def test_adjoint_matches_oracle(case, accum, monkeypatch):
+    """Both accumulations of the spray: 64-bit fixed-point windows into an FP64 data cube
+    (the default) and fp32 shared-memory atomics into an fp32 cube (PSM_ADJ_ACCUM=f32, read
+    when the context is created)."""
+    if accum == "f32":
+        monkeypatch.setenv("PSM_ADJ_ACCUM", "f32")
+    else:
+        monkeypatch.delenv("PSM_ADJ_ACCUM", raising=False)
     W, g, mig = _setup(case)
     rng = np.random.default_rng(8)
     im = rng.standard_normal((g.n_oi, g.n_ox, g.n_t)).astype(np.float32)
@@ -100,3 +108,32 @@ def test_lsm_cg_reduces_the_residual():
     assert m.shape == mtrue.shape and len(hist) == 11
     assert np.all(np.diff(hist) <= 1e-6 * hist[0])  # CGLS residuals do not increase
     assert hist[-1] < 0.9 * hist[0]
+
+
+def _dot_test(n, n_t, seed, compensated):
+    import dataclasses
+    from poststackmig3d_b200 import plan_geometry
+    g = plan_geometry(n, n, n_t, 0.002, 25.0, 25.0, 30.0, 2000.0, 0, 0, True)
+    g = dataclasses.replace(g, compensated=compensated)
+    vr = np.full((n, n, n_t), 2000.0, dtype=np.float32)
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal((n, n, n_t)).astype(np.float32)
+    im = rng.standard_normal((g.n_oi, g.n_ox, n_t)).astype(np.float32)
+    with Migrator(0) as mig:
+        mig.set_geometry(g)
+        mig.set_vrms(vr)
+        mig.set_traces(d)
+        Md = mig.forward()
+        MTm = mig.adjoint(im)
+    lhs = float(np.sum(Md.astype(np.float64) * im.astype(np.float64)))
+    rhs = float(np.sum(d.astype(np.float64) * MTm.astype(np.float64)))
+    return abs(lhs - rhs) / max(abs(lhs), abs(rhs))
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_dot_product_at_size(seed):
+    """The operator pair on 101x101 traces x 1001 samples (V 2000 m/s, 30 deg, amp on),
+    about 1e10 terms, where FP32 sums of thousands of terms per sample show: the adjoint
+    accumulates its windows as exact 64-bit integers and the data cube in FP64, and the
+    compensated forward sums its stages with Kahan's compensation."""
+    assert _dot_test(101, 1001, seed, compensated=True) <= 1e-5
