@@ -50,6 +50,13 @@ typedef enum { PSM_F32 = 0, PSM_BF16 = 1, PSM_F16 = 2 } psm_precision;
  *   compensated       nonzero: compensated (Kahan) summation over the aperture, partial
  *                     sums of at most 32 traces added with Kahan's compensation.  No
  *                     counterpart in the reference (plain fp32 sum, migration_kernel.cpp:229).
+ *   compat_omp_pad    0: padded output crosslines have v = 0 and are zero, as in the
+ *                     reference's serial build (migration_kernel.cpp:486-510).  Nonzero: the
+ *                     trailing padded crosslines are migrated with the last real crossline's
+ *                     Vrms (and their own position for r^2), which is what the reference's
+ *                     OpenMP build computes (its per-sample caches, :60-72, are not reset for
+ *                     crosslines with v = 0, and its nested crossline loop runs on one
+ *                     thread, src/main.cpp:255); Vrms is taken to be positive.
  */
 typedef struct {
     int32_t n_il, n_xl, n_t;
@@ -63,6 +70,7 @@ typedef struct {
     float tan2_theta;
     double dt_seconds;
     int32_t compensated;
+    int32_t compat_omp_pad;
 } psm_geom;
 
 typedef struct psm_ctx psm_ctx;

@@ -22,7 +22,9 @@ extern "C" {
  * NUL-terminated and truncated to the buffer size.  Keys beyond the reference's:
  *   precision   f32 | bf16 | f16   (default f32)  storage of the traces in HBM
  *   compensated bool              (default false) compensated summation
- *   device      int               (default 0)     CUDA device */
+ *   device      int               (default 0)     CUDA device
+ *   compat_omp_pad bool           (default false) trailing padded crosslines as the
+ *                                 reference's OpenMP build computes them (psm_geom) */
 typedef struct {
     char input_data[1024];
     char output_data[1024];
@@ -37,6 +39,7 @@ typedef struct {
     int32_t precision;
     int32_t compensated;
     int32_t device;
+    int32_t compat_omp_pad;
 } psm_config;
 
 /* ConfigParser::parseConfigFile followed by validateConfig. */

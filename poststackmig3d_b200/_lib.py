@@ -24,7 +24,7 @@ class PsmGeom(ctypes.Structure):
                 ("amp_correction", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("dt", ctypes.c_float), ("d_il", ctypes.c_float), ("d_xl", ctypes.c_float),
                 ("tan2_theta", ctypes.c_float), ("dt_seconds", ctypes.c_double),
-                ("compensated", ctypes.c_int32)]
+                ("compensated", ctypes.c_int32), ("compat_omp_pad", ctypes.c_int32)]
 
 
 class PsmProblem(ctypes.Structure):

@@ -105,6 +105,7 @@ Config parse_config(const std::string& path) {
             else throw Error("Cannot parse precision value: " + kv["precision"]);
         }
         if (kv.count("compensated")) c.compensated = to_bool(kv["compensated"]);
+        if (kv.count("compat_omp_pad")) c.compat_omp_pad = to_bool(kv["compat_omp_pad"]);
         if (kv.count("device")) c.device = to_int(kv["device"]);
     } catch (const Error& e) {
         throw Error(std::string("Error parsing config values: ") + e.what());

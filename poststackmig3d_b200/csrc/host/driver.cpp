@@ -191,6 +191,7 @@ void run(const Config& cfg, bool verbose, Plan* plan_only) {
         g.amp_correction = cfg.amp_correction ? 1 : 0;
         g.precision = cfg.precision;
         g.compensated = cfg.compensated ? 1 : 0;
+        g.compat_omp_pad = cfg.compat_omp_pad ? 1 : 0;
         g.dt = static_cast<float>(dt);
         g.d_il = static_cast<float>(cfg.inline_step);
         g.d_xl = static_cast<float>(cfg.crossline_step);

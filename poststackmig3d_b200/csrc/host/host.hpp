@@ -32,6 +32,7 @@ struct Config {  // include/config_parser.h:7-20 plus our extra keys
     int n_threads = 0;
     int precision = 0;  // 0 f32, 1 bf16, 2 f16
     bool compensated = false;
+    bool compat_omp_pad = false;  // trailing padded crosslines as the OpenMP build
     int device = 0;
 };
 

@@ -64,6 +64,7 @@ int psm_config_load(const char* path, psm_config* out, char* err, size_t err_len
         out->precision = c.precision;
         out->compensated = c.compensated;
         out->device = c.device;
+        out->compat_omp_pad = c.compat_omp_pad;
     });
 }
 

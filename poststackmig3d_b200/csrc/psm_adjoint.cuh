@@ -269,10 +269,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
     float gmax[2], gmin[2];
     float warpmax = -1.0f;
     const int x = x0 + warp - 1;
-    const int xv = x + P.xoff;
     if (warp > 0) {
-        const bool xvalid = x < P.n_ox && xv >= 0 && xv < P.n_vx;
-        const float* vp = vrms_trace(P, job.vrow, xvalid ? xv : 0);
+        const int vc = vrms_col(P, x);
+        const bool xvalid = vc >= 0;
+        const float* vp = vrms_trace(P, job.vrow, xvalid ? vc : 0);
         const float* mp = A.image + (static_cast<size_t>(jobi) * P.n_ox +
                                      (x < P.n_ox ? x : 0)) * P.n_t;
         float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
@@ -376,7 +376,8 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
             S.t0max = fmaxf(S.t0max, s.t0max);
         }
         const int xa = max(x0 + P.xoff, 0);
-        const int xb = min(min(x0 + kTX, P.n_ox) - 1 + P.xoff, P.n_vx - 1);
+        const int xb = min(min(x0 + kTX, P.n_ox) - 1 + P.xoff,
+                           P.compat_pad ? 0x3fffffff : P.n_vx - 1);
         int* inl_klo = reinterpret_cast<int*>(smem_raw + L.inl_klo);
         int* inl_pre = reinterpret_cast<int*>(smem_raw + L.inl_pre);
         float* inl_dx2 = reinterpret_cast<float*>(smem_raw + L.inl_dx2);

@@ -457,6 +457,7 @@ FwdParams volume_params(psm_ctx* c) {
     P.err = c->err.as<int>();
     P.wait_us = c->wait_us;
     P.fault = c->fault;
+    P.compat_pad = c->g.compat_omp_pad != 0;
     P.n_ci = c->g.n_il;
     P.n_cx = c->g.n_xl;
     P.n_t = c->g.n_t;
@@ -1983,6 +1984,7 @@ int psm_batch_create(psm_ctx* c, const psm_problem* problems, int n, psm_batch**
         P.err = c->err.as<int>();
         P.wait_us = c->wait_us;
         P.fault = c->fault;
+        P.compat_pad = g.compat_omp_pad != 0;
         P.n_ci = g.n_il;
         P.n_cx = g.n_xl;
         P.n_t = g.n_t;
@@ -2431,6 +2433,7 @@ extern "C" int psm_forward_noalloc(const psm_geom* g, const int32_t* out_center,
         }
     }
     FwdParams P{};
+    P.compat_pad = g->compat_omp_pad != 0;
     P.n_ci = g->n_il;
     P.n_cx = g->n_xl;
     P.n_t = g->n_t;

@@ -86,6 +86,7 @@ struct FwdParams {
     int* err;
     unsigned wait_us;  // limit of every mbarrier wait in microseconds (0: kDefaultWaitUs)
     int fault;         // test-only failure injection (kFault*), 0 normally
+    int compat_pad;    // trailing padded crosslines take the last real crossline's Vrms
     int n_ci, n_cx, n_t, ns;
     int n_vx;             // crosslines of a Vrms plane
     int n_ox;             // output crosslines per row
@@ -271,6 +272,21 @@ __device__ __forceinline__ float warp_min(float v) {
 // Vrms trace of output point (vrow, xv).
 __device__ __forceinline__ const float* vrms_trace(const FwdParams& P, int vrow, int xv) {
     return P.vrms + vrow * P.vs_row + xv * P.vs_x;
+}
+
+// Vrms crossline of output crossline x (cube crossline xv = x + xoff), or -1 when the point
+// has none: padded crosslines have v = 0 and no terms (migration_kernel.cpp:486-510, the
+// serial build).  With compat_pad, trailing padded crosslines take the last real crossline's
+// Vrms, as the reference's OpenMP build computes them: there the kernel's crossline loop is a
+// nested parallel region (src/main.cpp:255 already runs one output inline per thread), so
+// one thread walks every crossline in order, and its per-sample caches
+// (migration_kernel.cpp:60-72, :115-144), filled only where v >= 1e-5, still hold the last
+// real crossline's values, while r^2 is taken from the padded crossline's own position.
+__device__ __forceinline__ int vrms_col(const FwdParams& P, int x) {
+    const int xv = x + P.xoff;
+    if (x >= P.n_ox || xv < 0) return -1;
+    if (xv < P.n_vx) return xv;
+    return P.compat_pad ? P.n_vx - 1 : -1;
 }
 
 // Per output sample constants in the reference's FP32 order (migration_kernel.cpp:115-144).
@@ -739,10 +755,10 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
     float warpmax = -1.0f;
     float gminall = 3.0e38f;  // every lane of every group passes when r2 <= gminall
     const int x = x0 + warp - 1;
-    const int xv = x + P.xoff;
     if (warp > 0) {
-        const bool xvalid = x < P.n_ox && xv >= 0 && xv < P.n_vx;
-        const float* vp = vrms_trace(P, job.vrow, xvalid ? xv : 0);
+        const int vc = vrms_col(P, x);
+        const bool xvalid = vc >= 0;
+        const float* vp = vrms_trace(P, job.vrow, xvalid ? vc : 0);
         float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
         float bj[J];
 #pragma unroll
@@ -833,7 +849,8 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         }
         // cube crossline range of the tile's output points
         const int xa = max(x0 + P.xoff, 0);
-        const int xb = min(min(x0 + kTX, P.n_ox) - 1 + P.xoff, P.n_vx - 1);
+        const int xb = min(min(x0 + kTX, P.n_ox) - 1 + P.xoff,
+                           P.compat_pad ? 0x3fffffff : P.n_vx - 1);
         int* inl_klo = reinterpret_cast<int*>(smem_raw + L.inl_klo);
         int* inl_pre = reinterpret_cast<int*>(smem_raw + L.inl_pre);
         float* inl_dx2 = reinterpret_cast<float*>(smem_raw + L.inl_dx2);
@@ -1079,8 +1096,9 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
 
     // ---- write the tile: weight 1/(t v^2) = (dt/t) * inv_dt / v^2 applied per output sample
     if (x < P.n_ox) {
-        const bool xvalid = xv >= 0 && xv < P.n_vx;
-        const float* vp = vrms_trace(P, job.vrow, xvalid ? xv : 0);
+        const int vc = vrms_col(P, x);
+        const bool xvalid = vc >= 0;
+        const float* vp = vrms_trace(P, job.vrow, xvalid ? vc : 0);
         float* op = P.image + (static_cast<size_t>(job.row) * P.n_ox + x) * P.n_t;
 #pragma unroll
         for (int j = 0; j < J; ++j) {
@@ -1199,10 +1217,14 @@ __global__ void count_kernel(const FwdParams P, unsigned long long* out) {
     const int x = blockIdx.x;
     const Job job = P.jobs[blockIdx.y];
     const int xv = x + P.xoff;
+    // the farthest trace of the cube from crossline xv (xv >= 0; beyond n_cx - 1 with
+    // compat_pad), plus one
+    const int dcap = max(xv, P.n_cx - 1 - xv) + 1;
     unsigned long long local = 0;
     for (int t = threadIdx.x; t < P.n_t; t += blockDim.x) {
-        if (xv < 0 || xv >= P.n_vx) break;
-        const float v = vrms_trace(P, job.vrow, xv)[t];
+        const int vc = vrms_col(P, x);
+        if (vc < 0) break;
+        const float v = vrms_trace(P, job.vrow, vc)[t];
         const PointConst pc = point_const(v, P.t0[t], P.tan2);
         const float B = pass_bound(pc, P.inv_dt, P.ntm1f);
         if (B < 0.0f) continue;
@@ -1210,9 +1232,9 @@ __global__ void count_kernel(const FwdParams P, unsigned long long* out) {
             const float dx2 = inline_dx2(P.il_pos[i], job.pos, P.d_il);
             if (dx2 > B) continue;  // d = 0 passes from here on
             int d = static_cast<int>(sqrtf(fmaxf(B - dx2, 0.0f)) * P.inv_dxl);
-            d = min(d, P.n_cx + 1);
+            d = min(d, dcap);
             while (d > 0 && trace_r2(d, P.d_xl, dx2) > B) --d;
-            while (d <= P.n_cx && trace_r2(d + 1, P.d_xl, dx2) <= B) ++d;
+            while (d < dcap && trace_r2(d + 1, P.d_xl, dx2) <= B) ++d;
             const int lo = max(0, xv - d), hi = min(P.n_cx - 1, xv + d);
             if (hi >= lo) local += static_cast<unsigned long long>(hi - lo + 1);
         }

@@ -2,11 +2,13 @@
 // the device that runs them (psm_measure_limbs, include/psm.h).
 //
 // Each probe kernel runs a fixed number of independent operations per thread on every SM at
-// once (148 SMs x kCtasPerSm CTAs of kThreads threads, all resident together) and records the
-// SM-clock span of every CTA with clock64().  A rate per clock per SM is
-//     operations per SM / median CTA span (cycles),
-// which does not depend on the clock the GPU ran at; the clock itself is the span divided by
-// the CUDA-event time of the launch.  Every shared-memory index stays inside the CTA's static
+// once (148 SMs x kCtasPerSm CTAs of kThreads threads, all resident together) and records,
+// for every CTA, its SM and its first and last clock64() reading.  An SM's busy span is the
+// last end minus the first start over its CTAs (one SM clock counter), and a rate per clock
+// per SM is
+//     operations of the SM's CTAs / that span (cycles), median over the SMs,
+// which does not depend on the clock the GPU ran at; the clock itself is the median span
+// divided by the CUDA-event time of the launch.  Every shared-memory index stays inside the CTA's static
 // array, and every loop has a fixed trip count.
 #include <cuda_runtime.h>
 
@@ -25,9 +27,16 @@ __device__ __forceinline__ void span_begin(unsigned long long* t) {
     __syncthreads();
     if (threadIdx.x == 0) *t = clock64();
 }
+// spans[3 b .. 3 b + 2] = SM id, start, end of CTA b
 __device__ __forceinline__ void span_end(unsigned long long t0, unsigned long long* spans) {
     __syncthreads();
-    if (threadIdx.x == 0) spans[blockIdx.x] = clock64() - t0;
+    if (threadIdx.x == 0) {
+        unsigned smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        spans[3 * blockIdx.x] = smid;
+        spans[3 * blockIdx.x + 1] = t0;
+        spans[3 * blockIdx.x + 2] = clock64();
+    }
 }
 
 // 8 independent rsqrt chains per thread (MUFU.RSQ; the library builds with -ftz=true).
@@ -180,15 +189,16 @@ __global__ void __launch_bounds__(kThreads) iatom_probe(int iters, float* sink,
     if (sm[threadIdx.x] == static_cast<T>(12345)) sink[threadIdx.x] = 1.0f;
 }
 
-// Median CTA span (cycles) and event time (ms) of one launch of kernel k.
+// Median SM span (cycles), CTAs per SM that the spans cover, and event time (ms) of one
+// launch of kernel k.
 template <typename K>
-int time_probe(K k, int iters, int n_sm, double* cycles, double* ms) {
+int time_probe(K k, int iters, int n_sm, double* cycles, double* ms, double* ctas_per_sm) {
     const int n_cta = n_sm * kCtasPerSm;
     unsigned long long* spans = nullptr;
     float* sink = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int rc = PSM_OK;
-    if (cudaMalloc(&spans, sizeof(unsigned long long) * n_cta) != cudaSuccess ||
+    if (cudaMalloc(&spans, 3 * sizeof(unsigned long long) * n_cta) != cudaSuccess ||
         cudaMalloc(&sink, sizeof(float) * kThreads) != cudaSuccess ||
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         rc = PSM_ERR_NOMEM;
@@ -200,11 +210,35 @@ int time_probe(K k, int iters, int n_sm, double* cycles, double* ms) {
         if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
             rc = PSM_ERR_CUDA;
         } else {
-            std::vector<unsigned long long> h(n_cta);
-            cudaMemcpy(h.data(), spans, sizeof(unsigned long long) * n_cta,
+            std::vector<unsigned long long> h(3 * static_cast<size_t>(n_cta));
+            cudaMemcpy(h.data(), spans, 3 * sizeof(unsigned long long) * n_cta,
                        cudaMemcpyDeviceToHost);
-            std::nth_element(h.begin(), h.begin() + n_cta / 2, h.end());
-            *cycles = static_cast<double>(h[n_cta / 2]);
+            // per SM: first start, last end, CTAs
+            std::vector<unsigned long long> first(n_sm, ~0ull), last(n_sm, 0);
+            std::vector<int> count(n_sm, 0);
+            for (int b = 0; b < n_cta; ++b) {
+                const unsigned long long sm = h[3 * b];
+                if (sm >= static_cast<unsigned long long>(n_sm)) continue;
+                first[sm] = std::min(first[sm], h[3 * b + 1]);
+                last[sm] = std::max(last[sm], h[3 * b + 2]);
+                ++count[sm];
+            }
+            std::vector<double> span, per;
+            for (int sm = 0; sm < n_sm; ++sm)
+                if (count[sm] > 0 && last[sm] > first[sm]) {
+                    span.push_back(static_cast<double>(last[sm] - first[sm]) / count[sm]);
+                    per.push_back(count[sm]);
+                }
+            if (span.empty()) {
+                rc = PSM_ERR_CUDA;
+            } else {
+                // span per CTA of work, times the CTAs one SM ran: the cycles of kCtasPerSm
+                // CTAs' work on one SM
+                std::nth_element(span.begin(), span.begin() + span.size() / 2, span.end());
+                *cycles = span[span.size() / 2] * kCtasPerSm;
+                std::nth_element(per.begin(), per.begin() + per.size() / 2, per.end());
+                *ctas_per_sm = per[per.size() / 2];
+            }
             float t = 0.0f;
             cudaEventElapsedTime(&t, e0, e1);
             *ms = t;
@@ -227,41 +261,41 @@ extern "C" int psm_measure_limbs(int device, psm_limbs* out) {
         return PSM_ERR_CUDA;
     const double per_sm = static_cast<double>(kThreads) * kCtasPerSm;  // threads per SM
     constexpr int kIters = 1 << 14;
-    double cyc = 0.0, ms = 0.0, clk_sum = 0.0;
+    double cyc = 0.0, ms = 0.0, clk_sum = 0.0, cps = kCtasPerSm;
     int n_clk = 0;
     int rc;
     // rate per clock per SM of `ops` operations per thread
     auto rate = [&](double ops) {
-        clk_sum += cyc / (ms * 1e-3) / 1e6;
+        clk_sum += cyc / kCtasPerSm * cps / (ms * 1e-3) / 1e6;
         ++n_clk;
         return ops * per_sm / cyc;
     };
-    if ((rc = time_probe(rsq_probe, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(rsq_probe, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->rsqrt_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(ffma_probe, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(ffma_probe, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->ffma_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(ffma2_probe, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(ffma2_probe, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->ffma2_per_clk_sm = rate(16.0 * kIters);
-    if ((rc = time_probe(lds64_probe<false>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(lds64_probe<false>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->lds64_bytes_per_clk_sm = rate(64.0 * kIters);
-    if ((rc = time_probe(lds64_probe<true>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(lds64_probe<true>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->lds64_slope_bytes_per_clk_sm = rate(64.0 * kIters);
-    if ((rc = time_probe(atom_probe<false, false>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(atom_probe<false, false>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->atom_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(atom_probe<true, false>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(atom_probe<true, false>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->atom_slope_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(atom_probe<false, true>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(atom_probe<false, true>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->red_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(atom_probe<true, true>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(atom_probe<true, true>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->red_slope_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(iatom_probe<false, unsigned>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(iatom_probe<false, unsigned>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->atom_u32_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(iatom_probe<true, unsigned>, kIters, n_sm, &cyc, &ms))) return rc;
+    if ((rc = time_probe(iatom_probe<true, unsigned>, kIters, n_sm, &cyc, &ms, &cps))) return rc;
     out->atom_u32_slope_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(iatom_probe<false, unsigned long long>, kIters, n_sm, &cyc, &ms)))
+    if ((rc = time_probe(iatom_probe<false, unsigned long long>, kIters, n_sm, &cyc, &ms, &cps)))
         return rc;
     out->atom_u64_per_clk_sm = rate(8.0 * kIters);
-    if ((rc = time_probe(iatom_probe<true, unsigned long long>, kIters, n_sm, &cyc, &ms)))
+    if ((rc = time_probe(iatom_probe<true, unsigned long long>, kIters, n_sm, &cyc, &ms, &cps)))
         return rc;
     out->atom_u64_slope_per_clk_sm = rate(8.0 * kIters);
     out->sm_clock_mhz = clk_sum / n_clk;

@@ -22,7 +22,7 @@ class PsmConfig(ctypes.Structure):
                 ("velocity", ctypes.c_char * 1024), ("angle_aperture", ctypes.c_double),
                 ("amp_correction", ctypes.c_int32), ("n_threads", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("compensated", ctypes.c_int32),
-                ("device", ctypes.c_int32)]
+                ("device", ctypes.c_int32), ("compat_omp_pad", ctypes.c_int32)]
 
     def as_dict(self):
         d = {}
@@ -31,6 +31,7 @@ class PsmConfig(ctypes.Structure):
             d[name] = v.decode() if isinstance(v, bytes) else v
         d["amp_correction"] = bool(d["amp_correction"])
         d["compensated"] = bool(d["compensated"])
+        d["compat_omp_pad"] = bool(d["compat_omp_pad"])
         return d
 
 

@@ -109,6 +109,7 @@ class Geometry:
     amp: bool = True
     precision: str = "f32"
     compensated: bool = False
+    compat_omp_pad: bool = False  # trailing padded crosslines as the reference's OpenMP build
 
     @property
     def dt(self) -> float:
@@ -123,7 +124,8 @@ class Geometry:
         return PsmGeom(self.n_il, self.n_xl, self.n_t, self.pad_il, self.pad_xl, self.n_oi,
                        self.n_ox, self.m_il, int(bool(self.amp)), PRECISIONS[self.precision],
                        np.float32(self.dt_seconds), self.d_il, self.d_xl, self.tan2,
-                       self.dt_seconds, int(bool(self.compensated)))
+                       self.dt_seconds, int(bool(self.compensated)),
+                       int(bool(self.compat_omp_pad)))
 
 
 def plan_geometry(n_il: int, n_xl: int, n_t: int, dt_seconds: float, d_il: float,

@@ -66,3 +66,37 @@ def test_binary_reports_errors_like_the_reference(tmp_path):
     assert r.returncode == 1 and "Error: Cannot open SEGY file: nope.sgy" in r.stderr
     r = H.run_binary(str(tmp_path / "missing.txt"), timeout=60)
     assert r.returncode == 1 and "Error: Config file not found" in r.stderr
+
+
+def test_compat_omp_pad_matches_the_reference_openmp_binary(tmp_path):
+    """compat_omp_pad=true reproduces the reference's OpenMP build, trailing padded
+    crosslines included (there its per-sample caches keep the last real crossline's values,
+    migration_kernel.cpp:60-72); without it those crosslines are zero, as in the serial
+    build.  Every other trace is the same in both builds."""
+    import oracle as O
+    if not os.path.exists(O.ref_binary("omp")):
+        pytest.skip("the reference binary was not built")
+    W = S.random_workload(61, 11, 9, 160, vel_kind="lateral", pad_il=2, pad_xl=3, angle=40.0,
+                          dt=0.004)
+    ref_cfg = S.write_run(str(tmp_path), W, output="ref.sgy", n_threads=4)
+    rr = O.run_ref_binary(ref_cfg, "omp", timeout=600)
+    assert rr.returncode == 0, rr.stderr
+    ref = S.read_segy_raw(str(tmp_path / "ref.sgy"))
+    n_ox = 9 + 2 * 3
+    b = S.decode_samples(ref[3], 5).reshape(-1, n_ox, 160)
+    assert np.abs(b[:, -3:]).max() > 0  # the quirk shows in this case
+    for compat in (True, False):
+        cfg = S.write_run(str(tmp_path), W, output=f"ours{int(compat)}.sgy",
+                          compat_omp_pad=compat)
+        r = H.run_binary(cfg, timeout=300)
+        assert r.returncode == 0, r.stderr
+        got = S.read_segy_raw(str(tmp_path / f"ours{int(compat)}.sgy"))
+        assert got[0] == ref[0] and got[1] == ref[1] and np.array_equal(got[2], ref[2])
+        a = S.decode_samples(got[3], 5).reshape(-1, n_ox, 160)
+        if compat:
+            rms, mx = rel_err(a, b)
+            assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (rms, mx)
+        else:
+            assert not a[:, -3:].any()
+            rms, mx = rel_err(a[:, :-3], b[:, :-3])
+            assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (rms, mx)

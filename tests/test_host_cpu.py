@@ -75,6 +75,7 @@ def test_config_defaults(tmp_path):
     assert c["angle_aperture"] == 30.0 and c["amp_correction"] is True
     assert c["n_threads"] == 0 and c["velocity"] == "2000"
     assert c["precision"] == 0 and c["compensated"] is False and c["device"] == 0
+    assert c["compat_omp_pad"] is False
 
 
 def test_config_every_key_quotes_comments_duplicates(tmp_path):
@@ -82,7 +83,7 @@ def test_config_every_key_quotes_comments_duplicates(tmp_path):
             "inline_step=10\ninline_step=20\ncrossline_step=5.5m\nvelocity = v.sgy\n"
             "inline_padding=3\ncrossline_padding=4\nangle_aperture=45.5\n"
             "amp_correction=OFF\nn_threads=8\nunknown_key=whatever\nprecision=bf16\n"
-            "compensated=yes\ndevice=0\n")
+            "compensated=yes\ndevice=0\ncompat_omp_pad=on\n")
     c = H.load_config(_cfg(tmp_path, text))
     assert c["input_data"] == "a b.sgy" and c["output_data"] == "o.sgy"
     assert c["inline_step"] == 20.0          # last duplicate wins
@@ -91,6 +92,7 @@ def test_config_every_key_quotes_comments_duplicates(tmp_path):
     assert (c["inline_padding"], c["crossline_padding"]) == (3, 4)
     assert c["angle_aperture"] == 45.5 and c["amp_correction"] is False
     assert c["n_threads"] == 8 and c["precision"] == 1 and c["compensated"] is True
+    assert c["compat_omp_pad"] is True
 
 
 @pytest.mark.parametrize("spelling,value", [("true", True), ("1", True), ("Yes", True),
