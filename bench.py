@@ -569,12 +569,42 @@ def run_lsm(args):
     m.set_vrms(vr)
     d = m.adjoint(mtrue)
     d += (0.05 * np.abs(d).max() * rng.standard_normal(d.shape)).astype(np.float32)
-    # dot-product test of the operator pair on seeded random vectors
+    # dot-product test of the operator pair on seeded random vectors, with the plain and with
+    # the compensated forward; the error is also given relative to ||M d|| ||m||, which does
+    # not depend on how nearly orthogonal the two random vectors happen to be
     d1 = rng.standard_normal(d.shape).astype(np.float32)
     m1 = rng.standard_normal(mtrue.shape).astype(np.float32)
     m.set_traces(d1)
-    lhs = float(np.sum(m.forward().astype(np.float64) * m1))
-    rhs = float(np.sum(d1.astype(np.float64) * m.adjoint(m1)))
+    Md = m.forward()
+    MTm = m.adjoint(m1)
+    rhs = float(np.sum(d1.astype(np.float64) * MTm))
+    lhs = float(np.sum(Md.astype(np.float64) * m1))
+    norms = float(np.linalg.norm(Md.astype(np.float64)) * np.linalg.norm(m1.astype(np.float64)))
+    gk = dataclasses.replace(g, compensated=True)
+    m.set_geometry(gk)
+    m.set_vrms(vr)
+    m.set_traces(d1)
+    lhs_k = float(np.sum(m.forward().astype(np.float64) * m1))
+    m.set_geometry(g)
+    m.set_vrms(vr)
+    dot = {"plain_forward": abs(lhs - rhs) / max(abs(lhs), abs(rhs)),
+           "compensated_forward": abs(lhs_k - rhs) / max(abs(lhs_k), abs(rhs)),
+           "plain_vs_norms": abs(lhs - rhs) / norms,
+           "compensated_vs_norms": abs(lhs_k - rhs) / norms,
+           "cos": lhs / norms}
+    # one adjoint application with pinned host buffers (CUDA events; includes 0.33 GB of copies)
+    stream = torch.cuda.ExternalStream(m.stream_handle())
+    h_m1 = torch.from_numpy(m1).pin_memory()
+    h_out = torch.empty(d.shape, dtype=torch.float32).pin_memory()
+    m.adjoint(h_m1.numpy(), h_out.numpy())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        m.adjoint(h_m1.numpy(), h_out.numpy())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    adj_ms = e0.elapsed_time(e1) / 3
     iters = 10
     props = torch.cuda.get_device_properties(0)
     uuid = str(getattr(props, "uuid", ""))
@@ -594,7 +624,10 @@ def run_lsm(args):
                        "iterations": iters},
             "relative_residual": float(hist[-1] / hist[0]),
             "residual_history": [float(h / hist[0]) for h in hist],
-            "dot_product_rel_err": abs(lhs - rhs) / max(abs(lhs), abs(rhs)),
+            "dot_product_rel_err": dot["compensated_forward"],
+            "dot_product": dot,
+            "adjoint_ms_with_copies": adj_ms,
+            "adjoint_accumulation": os.environ.get("PSM_ADJ_ACCUM", "f32"),
             "dtype": "f32 operators, f64 CG scalars", "data": "synthetic (seeded)",
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -661,6 +694,8 @@ def run_batch(args):
     ms_sep = timed(max(1, min(args.steps, 3)))
     b.set_mode(Batch.PERSISTENT)
     ms_pers = timed(max(1, min(args.steps, 3)))
+    b.set_mode(Batch.ONE_GRID)
+    ms_grid = timed(max(1, min(args.steps, 3)))
     b.set_mode(chosen_mode)
     torch.cuda.synchronize()
     clk.start()
@@ -714,12 +749,14 @@ def run_batch(args):
                                    f"401-1001 samples, own linear Vrms",
                        "problems": len(probs), "n_terms": n_terms,
                        "storage": args.storage, "compensated": bool(args.compensated),
-                       "launch": ("one persistent launch per step" if chosen_mode == 0 else
-                                  "one grid launch per problem") + ", replayed as a CUDA graph "
-                                                                    "(autotuned schedule)",
+                       "launch": {0: "one persistent launch per step",
+                                  1: "one grid launch per problem",
+                                  2: "one grid launch over every problem's tiles"}[chosen_mode]
+                                 + ", replayed as a CUDA graph (autotuned schedule)",
                        "variant": Migrator.VARIANTS[b.variant()],
                        "tile_order": Batch.ORDERS[b.order()], "autotune_ms": tuned,
                        "per_problem_graph_ms": ms_sep, "persistent_graph_ms": ms_pers,
+                       "one_grid_graph_ms": ms_grid,
                        "l2": "inputs larger than L2 (panel cube 121 MB, images 3.9 GB)"},
             "roofline": {"bound": bound, "achieved": value, "peak": peak, "unit": "Gterm/s",
                          "frac": value / peak, "traffic": None, "limbs": limb_peaks,

@@ -288,7 +288,9 @@ typedef struct psm_batch psm_batch;
 
 typedef enum {
     PSM_BATCH_PERSISTENT = 0,  /* one persistent launch over every problem's tiles */
-    PSM_BATCH_PER_PROBLEM = 1  /* one grid launch per problem */
+    PSM_BATCH_PER_PROBLEM = 1, /* one grid launch per problem */
+    PSM_BATCH_ONE_GRID = 2     /* one grid launch over every problem's tiles, a CTA per tile in
+                                  the tile order (the block scheduler balances the load) */
 } psm_batch_mode;
 
 /* At most 184 problems (PSM_ERR_UNSUPPORTED beyond): their parameters travel as one kernel
@@ -313,9 +315,10 @@ typedef enum {
 } psm_tile_order;
 int psm_batch_set_order(psm_batch *batch, int order);
 int psm_batch_get_order(psm_batch *batch, int *order);
-/* Times one run per distinct kernel variant on each of three schedules (persistent
- * depth-first, persistent problem order, one launch per problem) and keeps the fastest
- * variant, order and mode; ms[3 * PSM_FWD_N_VARIANTS] (may be NULL) receives the times at
+/* Times one run per distinct kernel variant on each of five schedules (0 persistent
+ * depth-first, 1 persistent problem order, 2 one launch per problem, 3 one grid depth-first,
+ * 4 one grid problem order) and keeps the fastest
+ * variant, order and mode; ms[5 * PSM_FWD_N_VARIANTS] (may be NULL) receives the times at
  * [schedule * PSM_FWD_N_VARIANTS + variant], 0 for variants not run. */
 int psm_batch_autotune(psm_batch *batch, float *ms, int *best, int *best_order,
                        int *best_mode);

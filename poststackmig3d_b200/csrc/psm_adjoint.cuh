@@ -276,9 +276,16 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
         const float* mp = A.image + (static_cast<size_t>(jobi) * P.n_ox +
                                      (x < P.n_ox ? x : 0)) * P.n_t;
         float vmin = 3.0e38f, vmax = 0.0f, bmax = -1.0f, t0min = 3.0e38f, t0max = 0.0f;
+        // lane l holds samples T0 + 64 (j / 2) + 2 l + (j % 2): the 32 lanes of one block
+        // are two samples apart, so their trace samples (ds/dt0 = t0 / t >= cos(aperture)
+        // inside the aperture, 0.7 at 45 deg) fall on different window addresses, and the
+        // shared-memory atomics of one instruction do not collide (the forward's mapping,
+        // consecutive samples across lanes, puts about one lane in five on its neighbour's
+        // address, which halves the atomics' rate); groups of 4 blocks still span 128
+        // consecutive samples
 #pragma unroll
         for (int j = 0; j < kJ; ++j) {
-            const int t = T0 + 32 * j + lane;
+            const int t = T0 + 64 * (j >> 1) + 2 * lane + (j & 1);
             float v = 0.0f, t0v = 0.0f, mv = 0.0f;
             if (xvalid && t < P.n_t) {
                 v = __ldg(vp + t);

@@ -415,7 +415,7 @@ struct psm_ctx {
     DevBuf str_tr, str_v, str_img[2];
     cudaEvent_t ev_placed = nullptr, ev_staged = nullptr, ev_done[2] = {nullptr, nullptr};
     // adjoint: 64-bit fixed-point window sums and an FP64 data cube (else fp32 atomics)
-    bool adj_fixed = true;
+    bool adj_fixed = false;
     DevBuf adj64;
     // limit of the kernels' mbarrier waits (us; 0: the kernels' default of 4 s) and the
     // test-only failure injection (psm::kFault*), both read from the environment by psm_create
@@ -436,8 +436,8 @@ void read_fault_env(psm_ctx* c) {
         const long long ms = std::atoll(w);
         if (ms > 0 && ms < 4000000) c->wait_us = static_cast<unsigned>(ms * 1000);
     }
-    if (const char* a = std::getenv("PSM_ADJ_ACCUM"))  // "f32": fp32 atomics in the adjoint
-        c->adj_fixed = std::strcmp(a, "f32") != 0;
+    if (const char* a = std::getenv("PSM_ADJ_ACCUM"))  // "fixed": 64-bit fixed-point sums
+        c->adj_fixed = std::strcmp(a, "fixed") == 0;
     if (const char* f = std::getenv("PSM_FAULT")) {
         if (!std::strcmp(f, "stall_producer")) c->fault = psm::kFaultStallProducer;
         if (!std::strncmp(f, "nomem:", 6)) g_fail_alloc.store(std::atoi(f + 6));
@@ -1753,6 +1753,39 @@ cudaError_t launch_persistent(K, const psm_batch& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// The one-grid kernel K (a CTA per tile of the list): its shared-memory attribute, set before
+// a stream capture.
+template <class K>
+cudaError_t prepare_items(K, const psm_batch& b) {
+    auto* kern = psm::fwd_items_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN,
+                                       K::PAIRS, K::MINB>;
+    const size_t smem =
+        psm::smem_layout(b.max_inl, persistent_stage_cap<K>(b), psm::store_bytes(K::STORE))
+            .total;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem));
+}
+
+template <class K>
+cudaError_t launch_items(K, const psm_batch& b, cudaStream_t s) {
+    auto* kern = psm::fwd_items_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN,
+                                       K::PAIRS, K::MINB>;
+    const int cap = persistent_stage_cap<K>(b);
+    const size_t smem = psm::smem_layout(b.max_inl, cap, psm::store_bytes(K::STORE)).total;
+    const int w = (K::J == 16 ? 2 : 0) + b.order;
+    if (b.n_items[w] <= 0) return cudaSuccess;
+    const psm::BatchParams* params = b.params.get();
+    std::unique_ptr<psm::BatchParams> small;
+    if constexpr (K::MINB > 2) {  // every problem stages into the smaller stages
+        small = std::make_unique<psm::BatchParams>(*b.params);
+        for (size_t i = 0; i < b.probs.size(); ++i) small->p[i].stage_cap = cap;
+        params = small.get();
+    }
+    kern<<<b.n_items[w], 32 * (psm::kTX + 1), smem, s>>>(
+        *params, b.items[w].as<psm::BatchItem>(), b.max_inl, cap);
+    return cudaGetLastError();
+}
+
 // Repeated output rows of every problem (padded output inlines, main.cpp:268-285).
 cudaError_t batch_copies(const psm_batch& b, cudaStream_t s) {
     for (const BatchProblem& p : b.probs) {
@@ -1772,7 +1805,11 @@ cudaError_t batch_copies(const psm_batch& b, cudaStream_t s) {
 cudaError_t batch_enqueue(psm_batch& b, int variant, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(b.ctx->err.p, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
-    if (b.mode == PSM_BATCH_PER_PROBLEM) {
+    if (b.mode == PSM_BATCH_ONE_GRID) {
+        e = with_kernel(b.amp, variant, b.store, b.kahan,
+                        [&](auto k) { return launch_items(k, b, s); });
+        if (e != cudaSuccess) return e;
+    } else if (b.mode == PSM_BATCH_PER_PROBLEM) {
         for (const BatchProblem& p : b.probs) {
             e = launch_fwd(p.P, static_cast<int>(p.jobs.size()), b.amp, variant, s, b.store,
                            b.kahan);
@@ -1793,13 +1830,17 @@ cudaError_t batch_enqueue(psm_batch& b, int variant, cudaStream_t s) {
 int batch_launch(psm_batch* b) {
     psm_ctx* c = b->ctx;
     const int v = effective_variant(b->variant, b->store, b->kahan);
-    const int key = (v * 2 + b->order) * 2 + b->mode;
+    const int key = (v * 2 + b->order) * 3 + b->mode;
     if (!b->exec || b->exec_key != key) {
         if (b->exec) {
             cudaGraphExecDestroy(b->exec);
             b->exec = nullptr;
         }
-        if (b->mode == PSM_BATCH_PERSISTENT)
+        if (b->mode == PSM_BATCH_ONE_GRID)
+            PSM_CUDA_TRY(c->st, with_kernel(b->amp, v, b->store, b->kahan, [&](auto k) {
+                             return prepare_items(k, *b);
+                         }));
+        else if (b->mode == PSM_BATCH_PERSISTENT)
             PSM_CUDA_TRY(c->st, with_kernel(b->amp, v, b->store, b->kahan, [&](auto k) {
                              return prepare_persistent(k, *b);
                          }));
@@ -2058,7 +2099,7 @@ int psm_batch_get_mode(psm_batch* b, int* mode) {
 }
 
 int psm_batch_set_mode(psm_batch* b, int mode) {
-    if (!b || (mode != PSM_BATCH_PERSISTENT && mode != PSM_BATCH_PER_PROBLEM))
+    if (!b || mode < PSM_BATCH_PERSISTENT || mode > PSM_BATCH_ONE_GRID)
         return PSM_ERR_ARG;
     b->mode = mode;
     return PSM_OK;
@@ -2109,7 +2150,7 @@ int psm_batch_autotune(psm_batch* b, float* ms, int* best, int* best_order, int*
     psm_ctx* c = b->ctx;
     cudaSetDevice(c->device);
     if (ms)
-        for (int v = 0; v < 3 * PSM_FWD_N_VARIANTS; ++v) ms[v] = 0.0f;
+        for (int v = 0; v < 5 * PSM_FWD_N_VARIANTS; ++v) ms[v] = 0.0f;
     cudaEvent_t e0, e1;
     PSM_CUDA_TRY(c->st, cudaEventCreate(&e0));
     PSM_CUDA_TRY(c->st, cudaEventCreate(&e1));
@@ -2117,10 +2158,12 @@ int psm_batch_autotune(psm_batch* b, float* ms, int* best, int* best_order, int*
     int pick_order = b->order, pick_mode = b->mode;
     float pick_ms = 3.0e38f;
     int rc = PSM_OK;
-    // schedules: persistent depth-first, persistent problem order, one launch per problem
-    for (int sch = 0; sch < 3 && rc == PSM_OK; ++sch) {
-        b->mode = sch < 2 ? PSM_BATCH_PERSISTENT : PSM_BATCH_PER_PROBLEM;
-        b->order = sch < 2 ? sch : PSM_ORDER_DEPTH_FIRST;
+    // schedules: persistent depth-first / problem order, one launch per problem, one grid
+    // depth-first / problem order
+    for (int sch = 0; sch < 5 && rc == PSM_OK; ++sch) {
+        b->mode = sch < 2 ? PSM_BATCH_PERSISTENT
+                          : (sch == 2 ? PSM_BATCH_PER_PROBLEM : PSM_BATCH_ONE_GRID);
+        b->order = sch < 2 ? sch : (sch == 2 ? PSM_ORDER_DEPTH_FIRST : sch - 3);
         for (int v = 1; v < PSM_FWD_N_VARIANTS && rc == PSM_OK; ++v) {
             if (effective_variant(v, b->store, b->kahan) != v) continue;  // same kernel
             b->variant = v;

@@ -726,6 +726,11 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
 // per CTA (ring_init); it counts the ring stages the CTA has used so far, so consecutive tiles
 // of a persistent CTA continue the ring's phases (every stage, the end-of-stream marker
 // included, is released by the consumers).  Returns false when a bounded wait expired.
+// One tile of a batched launch: problem, job of that problem, first crossline and sample.
+struct BatchItem {
+    int prob, job, x0, T0;
+};
+
 template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false>
 __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int x0, int T0,
                                          unsigned char* smem_raw, const SmemLayout& L,
@@ -1158,10 +1163,6 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdPara
         P, P.jobs[blockIdx.z], blockIdx.x * kTX, blockIdx.y * 32 * J, smem_raw, L, it);
 }
 
-// One tile of a batched launch: problem, job of that problem, first crossline and sample.
-struct BatchItem {
-    int prob, job, x0, T0;
-};
 
 // Parameters of every problem of a batched launch, passed by value: they live in the
 // kernel-parameter constant bank, whose loads are cached and uniform across the CTA.
@@ -1204,6 +1205,24 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB)
         // barrier: the tile's tables, statistics, s_item and s_job are reused next
         if (__syncthreads_or(!ok)) break;
     }
+}
+
+// The same tile list in ONE grid launch: CTA b migrates tile items[b] (deepest tiles first in
+// the depth-first order), and the hardware's block scheduler hands tiles to SMs as others
+// finish, so the CTAs carry no state from tile to tile.
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
+          bool PAIRS = false, int MINB = 2>
+__global__ void __launch_bounds__(32 * (kTX + 1), MINB)
+    fwd_items_kernel(const __grid_constant__ BatchParams B, const BatchItem* __restrict__ items,
+                     int max_inl, int stage_cap) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const SmemLayout L = smem_layout(max_inl, stage_cap, store_bytes(STORE));
+    if (threadIdx.x == 0) ring_init(smem_raw, L);
+    const BatchItem w = items[blockIdx.x];
+    const FwdParams& P = B.p[w.prob];
+    uint32_t it = 0;
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(P, P.jobs[w.job], w.x0, w.T0, smem_raw,
+                                                      L, it);
 }
 
 // ----------------------------------------------------------------------------- term count

@@ -498,7 +498,7 @@ class Batch:
     psm_batch_*).  The host arrays of the problems are kept referenced: reload() uploads
     them again."""
 
-    PERSISTENT, PER_PROBLEM = 0, 1
+    PERSISTENT, PER_PROBLEM, ONE_GRID = 0, 1, 2
     DEPTH_FIRST, PROBLEM_ORDER = 0, 1
     ORDERS = {0: "depth-first", 1: "problem"}
 
@@ -557,7 +557,8 @@ class Batch:
         check(self._L.psm_batch_get_order(self._b, ctypes.byref(o)), self._m._err)
         return o.value
 
-    SCHEDULES = {0: "persistent/depth-first", 1: "persistent/problem", 2: "per-problem"}
+    SCHEDULES = {0: "persistent/depth-first", 1: "persistent/problem", 2: "per-problem",
+                 3: "one-grid/depth-first", 4: "one-grid/problem"}
 
     def mode(self) -> int:
         v = ctypes.c_int()
@@ -565,17 +566,17 @@ class Batch:
         return v.value
 
     def autotune(self):
-        """Time every kernel variant on each schedule (persistent depth-first, persistent
-        problem order, per-problem launches); keep the fastest.
-        Returns (variant, order, mode, {(variant, schedule): ms})."""
+        """Time every kernel variant on each schedule (SCHEDULES: persistent depth-first /
+        problem order, per-problem launches, one grid depth-first / problem order); keep the
+        fastest.  Returns (variant, order, mode, {(variant, schedule): ms})."""
         nv = max(Migrator.VARIANTS) + 1
-        ms = np.zeros(3 * nv, dtype=np.float32)
+        ms = np.zeros(5 * nv, dtype=np.float32)
         best, order, mode = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(self._L.psm_batch_autotune(self._b, ms.ctypes.data, ctypes.byref(best),
                                          ctypes.byref(order), ctypes.byref(mode)),
               self._m._err)
         return best.value, order.value, mode.value, {
-            (v, sch): float(ms[sch * nv + v]) for sch in (0, 1, 2) for v in Migrator.VARIANTS
+            (v, sch): float(ms[sch * nv + v]) for sch in range(5) for v in Migrator.VARIANTS
             if ms[sch * nv + v] > 0}
 
     def reload(self) -> None:

@@ -55,7 +55,9 @@ def _single(W, g, variant=0):
 @pytest.mark.parametrize("variant", [0, 5, 1])
 @pytest.mark.parametrize("mode,order", [(Batch.PERSISTENT, Batch.DEPTH_FIRST),
                                         (Batch.PERSISTENT, Batch.PROBLEM_ORDER),
-                                        (Batch.PER_PROBLEM, Batch.DEPTH_FIRST)])
+                                        (Batch.PER_PROBLEM, Batch.DEPTH_FIRST),
+                                        (Batch.ONE_GRID, Batch.DEPTH_FIRST),
+                                        (Batch.ONE_GRID, Batch.PROBLEM_ORDER)])
 def test_batch_matches_single_problem_runs(mode, order, variant):
     probs = _problems()
     singles = [_single(W, g, variant) for W, g, _ in probs]
