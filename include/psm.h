@@ -219,6 +219,11 @@ int psm_set_image(psm_ctx *ctx, const float *image);
  * resident traces with nothing (they stay). */
 int psm_adjoint(psm_ctx *ctx, const float *image, float *data);
 
+/* psm_adjoint on device memory, enqueued on the ctx stream: M^T of the ctx image
+ * (psm_image_device; after psm_set_image or a forward) into the ctx's fp32 trace cube, which
+ * psm_get_traces then reads.  Before the next forward, upload traces again. */
+int psm_adjoint_async(psm_ctx *ctx);
+
 /* Least-squares migration: `iters` iterations of CG (CGLS) on min ||M^T m - data||^2 from
  * m = 0, with FP32 operators and FP64 inner products and step lengths computed on the GPU.
  * data [n_il][n_xl][n_t] (host) in, image [n_oi][n_ox][n_t] (host) out, resid[iters + 1]

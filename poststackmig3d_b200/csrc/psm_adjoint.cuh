@@ -169,6 +169,43 @@ __device__ __forceinline__ void adj_term(unsigned char* sbase, float r2, uint32_
 
 // One slot for one consumer warp: the groups of blocks where some lane passes, without masks
 // where every lane of the group passes.
+// Two terms of one lane for a slot: samples t and t + 1 (blocks j and j + 1), fp32 sums.
+// With ds/dt0 <= 1 their floor(s) are equal or adjacent, so their four shares fall on at
+// most three window addresses: lo_a (c0_a), lo_a + 1 (c1_a, and c0_b when lo_b = lo_a + 1),
+// lo_a + 2 (c1_b); the lane adds the shares that meet in registers first and issues three
+// atomics where the two terms alone would issue four (two when lo_b = lo_a).  A term that
+// fails the masks (MASK) contributes nothing and its address is never used; lo_b beyond
+// lo_a + 1 (a steep Vrms) takes its own two atomics.
+template <bool AMP, bool MASK>
+__device__ __forceinline__ void adj_term2(unsigned char* sbase, float r2, uint32_t base,
+                                          float smax, float T2a, float F4a, float BBa,
+                                          float MKa, float T2b, float F4b, float BBb,
+                                          float MKb) {
+    const float2 t2 = fma2(make_float2(F4a, F4b), make_float2(r2, r2), make_float2(T2a, T2b));
+    const float qa = rsqrtf(t2.x), qb = rsqrtf(t2.y);
+    const float sa = fminf(t2.x * qa, smax), sb = fminf(t2.y * qb, smax);
+    const float ma = __fadd_rd(sa, 8388608.0f), mb = __fadd_rd(sb, 8388608.0f);
+    const float fa = sa - (ma - 8388608.0f), fb = sb - (mb - 8388608.0f);
+    const bool oka = !MASK || r2 <= BBa, okb = !MASK || r2 <= BBb;
+    if (MASK && !oka && !okb) return;
+    const float ca = AMP ? MKa * qa : MKa, cb = AMP ? MKb * qb : MKb;
+    const float c1a = oka ? ca * fa : 0.0f, c0a = oka ? ca - ca * fa : 0.0f;
+    const float c1b = okb ? cb * fb : 0.0f, c0b = okb ? cb - cb * fb : 0.0f;
+    const uint32_t la = __float_as_uint(ma), lb = __float_as_uint(mb);  // 2^23 + floor(s)
+    const uint32_t l0 = oka ? la : lb;  // the first address the lane adds to
+    const uint32_t d = lb - l0;         // 0, 1, or more (only when both pass)
+    float* p = reinterpret_cast<float*>(sbase + (base + (l0 << 2)));
+    const bool far = okb && d > 1u;
+    atomicAdd(p, c0a + (okb && d == 0u ? c0b : 0.0f));
+    atomicAdd(p + 1, c1a + (okb && d == 0u ? c1b : 0.0f) + (okb && d == 1u ? c0b : 0.0f));
+    if (okb && d == 1u) atomicAdd(p + 2, c1b);
+    if (far) {
+        float* q = reinterpret_cast<float*>(sbase + (base + (lb << 2)));
+        atomicAdd(q, c0b);
+        atomicAdd(q + 1, c1b);
+    }
+}
+
 template <bool AMP, bool FIX>
 __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2, uint32_t base,
                                           float smax,
@@ -178,16 +215,28 @@ __device__ __forceinline__ void adj_visit(unsigned char* sbase, float r2, uint32
 #pragma unroll
     for (int gr = 0; gr < 2; ++gr) {
         if (r2 <= gmax[gr]) {
-            if (r2 <= gmin[gr]) {
+            if (FIX) {  // exact integer shares: each term on its own
+                if (r2 <= gmin[gr]) {
 #pragma unroll
-                for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, false, FIX>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
-                                              MK[j]);
+                    for (int j = 4 * gr; j < 4 * gr + 4; ++j)
+                        adj_term<AMP, false, FIX>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
+                                                  MK[j]);
+                } else {
+#pragma unroll
+                    for (int j = 4 * gr; j < 4 * gr + 4; ++j)
+                        adj_term<AMP, true, FIX>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
+                                                 MK[j]);
+                }
+            } else if (r2 <= gmin[gr]) {  // blocks j, j + 1 hold samples t, t + 1
+#pragma unroll
+                for (int j = 4 * gr; j < 4 * gr + 4; j += 2)
+                    adj_term2<AMP, false>(sbase, r2, base, smax, T2[j], F4[j], BB[j], MK[j],
+                                          T2[j + 1], F4[j + 1], BB[j + 1], MK[j + 1]);
             } else {
 #pragma unroll
-                for (int j = 4 * gr; j < 4 * gr + 4; ++j)
-                    adj_term<AMP, true, FIX>(sbase, r2, base, smax, T2[j], F4[j], BB[j],
-                                             MK[j]);
+                for (int j = 4 * gr; j < 4 * gr + 4; j += 2)
+                    adj_term2<AMP, true>(sbase, r2, base, smax, T2[j], F4[j], BB[j], MK[j],
+                                         T2[j + 1], F4[j + 1], BB[j + 1], MK[j + 1]);
             }
         }
     }

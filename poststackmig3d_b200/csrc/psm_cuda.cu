@@ -1275,6 +1275,19 @@ int psm_adjoint(psm_ctx* c, const float* image, float* data) {
     return read_device_error(c);
 }
 
+int psm_adjoint_async(psm_ctx* c) {
+    if (!c) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry and vrms must be set");
+    cudaSetDevice(c->device);
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    int r = adjoint_dev(c, c->image.as<float>(), c->data.as<float>());
+    if (r) return r;
+    c->have_traces = false;      // the staged storage still holds the earlier traces
+    c->traces_readable = true;   // the fp32 cube holds M^T image
+    return PSM_OK;
+}
+
 int psm_lsm_cg(psm_ctx* c, const float* data, float* image, int iters, double* resid) {
     if (!c || !data || !image || iters < 0) return PSM_ERR_ARG;
     if (!c->have_geom || !c->have_vrms)

@@ -420,6 +420,11 @@ class Migrator:
         check(self._L.psm_adjoint(self._ctx, _addr(image), _addr(out)), self._err)
         return out
 
+    def adjoint_async(self) -> None:
+        """M^T of the ctx image into the ctx's trace cube, enqueued on the ctx stream
+        (psm_adjoint_async); get_traces() reads the result."""
+        check(self._L.psm_adjoint_async(self._ctx), self._err)
+
     def lsm_cg(self, data, iters: int):
         """Least-squares migration: CG on min ||M^T m - data||^2 (FP32 operators, FP64
         inner products on the GPU).  Returns (image, data-residual norms [iters + 1])."""
