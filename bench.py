@@ -635,7 +635,7 @@ def run_lsm(args):
                        "iterations": iters},
             "relative_residual": float(hist[-1] / hist[0]),
             "residual_history": [float(h / hist[0]) for h in hist],
-            "dot_product_rel_err": dot["compensated_forward"],
+            "dot_product_rel_err": dot["plain_forward"],
             "dot_product": dot,
             "operators": {
                 "terms_per_application": n_terms, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
