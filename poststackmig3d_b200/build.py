@@ -59,9 +59,11 @@ def build_cuda(force: bool = False, extra=()) -> str:
     or a header changed), then nvcc links the objects into lib/libpsm_cuda.so."""
     from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB, exist_ok=True)
+    out = os.path.join(LIB, "libpsm_cuda.so")
+    if not force and not extra and not _stale(out, CUDA_DEPS):
+        return out  # newer than every source (the objects need not be present)
     obj_dir = os.path.join(PKG, "_build", "debug" if extra else "release")
     os.makedirs(obj_dir, exist_ok=True)
-    out = os.path.join(LIB, "libpsm_cuda.so")
     objs = [os.path.join(obj_dir, os.path.basename(s)[:-3] + ".o") for s in CUDA_SRC]
     todo = [(s, o) for s, o in zip(CUDA_SRC, objs)
             if force or _stale(o, [s] + CUDA_HDR)]
