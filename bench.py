@@ -255,6 +255,15 @@ def cpu_reference_sample(W, g, rows, threads):
     return terms, secs, kind, out
 
 
+def _err(a, b):
+    """Relative RMS error of a against b, and max error relative to b's peak."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = float(np.sqrt(np.mean(b * b))) or 1.0
+    return {"rel_rms": float(np.sqrt(np.mean((a - b) ** 2)) / den),
+            "max_rel": float(np.abs(a - b).max() / (np.abs(b).max() or 1.0))}
+
+
 def parity_block(W, g, image, rows, ref_rows, threads):
     """Error of the GPU image on output rows `rows` against the reference's own kernel
     (ref_rows, FP32) and against the FP64 oracle of the same operator (fed the dequantised
@@ -262,13 +271,7 @@ def parity_block(W, g, image, rows, ref_rows, threads):
     peak of the rows."""
     import oracle as O
 
-    def err(a, b):
-        a = np.asarray(a, dtype=np.float64)
-        b = np.asarray(b, dtype=np.float64)
-        den = float(np.sqrt(np.mean(b * b))) or 1.0
-        return {"rel_rms": float(np.sqrt(np.mean((a - b) ** 2)) / den),
-                "max_rel": float(np.abs(a - b).max() / (np.abs(b).max() or 1.0))}
-
+    err = _err
     got = image[rows]
     data = W.data if g.precision == "f32" else O.dequantized(W.data, g.precision)
     sub = np.ascontiguousarray(g.out_center[rows])
@@ -756,6 +759,43 @@ def run_batch(args):
     clocks = clk.summary()
     from poststackmig3d_b200.migration import measure_limbs
     limbs = measure_limbs(0)
+
+    # parity of sampled rows: the slowest and fastest panels and the first sub-volume,
+    # against the reference's kernel (constant or linear Vrms, as the problem has) and the
+    # FP64 oracle; 16-bit storage is compared with the oracle fed the dequantised samples
+    parity = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+        threads = os.cpu_count() or 1
+        b.run()
+        checks = []
+        for k in (0, len(panels) - 1, len(panels)):
+            if k >= len(probs):
+                continue
+            p = probs[k]
+            W = panels[k] if k < len(panels) else subs[k - len(panels)]
+            gk = p.geom
+            row = [gk.n_oi // 2]
+            vr = W.vrms_cube()
+            img = b.image(k)[row]
+            data = W.data if args.storage == "f32" else O.dequantized(W.data, args.storage)
+            sub = np.ascontiguousarray(np.asarray(gk.out_center)[row])
+            _, r64, _ = O.migrate_volume(data, vr, sub, gk.n_ox, 0, 0, gk.m_il,
+                                         np.float32(gk.dt_seconds), gk.t0(),
+                                         np.float32(gk.tan2), gk.d_il, gk.d_xl, gk.amp,
+                                         O.CONTRACT | O.F64, threads, True)
+            e = {"problem": k, "row": row[0], "vs_fp64": _err(img, r64)}
+            if O.ref_available():
+                ref, _ = O.reference_rows(W.data, vr, gk.out_center, row, gk.n_ox, 0, 0,
+                                          gk.m_il, gk.dt_seconds, gk.t0(), gk.tan2, gk.d_il,
+                                          gk.d_xl, gk.amp)
+                e["vs_reference"] = _err(img, ref)
+            checks.append(e)
+        parity = {"checks": checks,
+                  "reference": "kirchhoffKernel3DWithPadding compiled from the reference's "
+                               "sources (oracle/_ref, OpenMP build)",
+                  "fp64": "FP64 oracle of the same operator" + (
+                      ", fed the dequantised samples" if args.storage != "f32" else "")}
     sm_mhz = clocks["sm_mhz"] or limbs["sm_clock_mhz"]
     bound, peak, limb_peaks = limb_roofline(limbs, sm_mhz, value,
                                             "pairs" in Migrator.VARIANTS[b.variant()],
@@ -784,7 +824,8 @@ def run_batch(args):
                          "peak_basis": f"measured limbs (psm_measure_limbs) x "
                                        f"{limbs['n_sm']} SMs x median SM clock "
                                        f"{sm_mhz:.0f} MHz under load"},
-            "cpu_baseline": None, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks}
+            "parity": parity, "cpu_baseline": None, "e2e": e2e, "gpu_launches": args.steps,
+            "clocks": clocks}
     print(json.dumps(line), flush=True)
     b.close()
     m.close()
