@@ -395,6 +395,7 @@ struct psm_ctx {
     // adjoint: rows of each job (fold of duplicated output rows), image upload, job images
     std::vector<int> fold_map, fold_off;
     DevBuf d_fold_map, d_fold_off, img_in, fold;
+    DevBuf d_copies;  // the repeated output rows as int2 (dst row, src row)
     // least-squares migration vectors: data space [n_tr][ns], image space [n_oi][n_ox][n_t]
     DevBuf cg_d, cg_r, cg_q, cg_m, cg_s, cg_p, cg_sc, cg_hist;
     // SEG-Y codec: the input trace records as uploaded, their cube positions, the output
@@ -442,6 +443,17 @@ void read_fault_env(psm_ctx* c) {
         if (!std::strcmp(f, "stall_producer")) c->fault = psm::kFaultStallProducer;
         if (!std::strncmp(f, "nomem:", 6)) g_fail_alloc.store(std::atoi(f + 6));
     }
+}
+
+// The repeated output rows of the ctx geometry, copied within image `img` in one launch.
+cudaError_t copy_rows(psm_ctx* c, float* img, cudaStream_t s) {
+    if (c->copies.empty()) return cudaSuccess;
+    const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
+    const size_t total = c->copies.size() * row;
+    const unsigned blocks = static_cast<unsigned>(std::min<size_t>((total + 255) / 256, 148 * 16));
+    psm::copy_rows_kernel<<<blocks, 256, 0, s>>>(img, c->d_copies.as<int2>(),
+                                                  static_cast<int>(c->copies.size()), row);
+    return cudaGetLastError();
 }
 
 FwdParams volume_params(psm_ctx* c) {
@@ -537,6 +549,7 @@ int psm_destroy(psm_ctx* c) {
     if (c->d2h_stream) cudaStreamDestroy(c->d2h_stream);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     c->d_jobs_waves.release();
+    c->d_copies.release();
     for (DevBuf* b : {&c->str_tr, &c->str_v, &c->str_img[0], &c->str_img[1], &c->adj64})
         b->release();
     for (cudaEvent_t e : {c->ev_placed, c->ev_staged, c->ev_done[0], c->ev_done[1]})
@@ -622,6 +635,12 @@ int psm_set_geometry(psm_ctx* c, const psm_geom* g, const int32_t* out_center) {
     PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_fold_off.p, c->fold_off.data(),
                                         c->fold_off.size() * sizeof(int),
                                         cudaMemcpyHostToDevice, c->stream));
+    std::vector<int2> cps;
+    for (const auto& cp : c->copies) cps.push_back(make_int2(cp.first, cp.second));
+    PSM_CUDA_TRY(c->st, c->d_copies.ensure(std::max<size_t>(cps.size(), 1) * sizeof(int2)));
+    if (!cps.empty())
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->d_copies.p, cps.data(), cps.size() * sizeof(int2),
+                                            cudaMemcpyHostToDevice, c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     c->have_geom = true;
     c->have_traces = c->have_vrms = c->traces_readable = false;
@@ -879,12 +898,7 @@ int psm_forward_async(psm_ctx* c) {
                                    c->g.amp_correction != 0, c->variant, c->stream, c->store,
                                    c->g.compensated != 0));
     // padded output inlines repeat the migrated edge inline (main.cpp:268-285)
-    const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
-    for (const auto& cp : c->copies)
-        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.as<float>() + cp.first * row,
-                                            c->image.as<float>() + cp.second * row,
-                                            row * sizeof(float), cudaMemcpyDeviceToDevice,
-                                            c->stream));
+    PSM_CUDA_TRY(c->st, copy_rows(c, c->image.as<float>(), c->stream));
     return PSM_OK;
 }
 
@@ -1235,11 +1249,7 @@ int forward_dev(psm_ctx* c, const float* d_vec, float* d_img) {
     PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
                                    c->g.amp_correction != 0, c->variant, c->stream,
                                    psm::kStoreF32, c->g.compensated != 0));
-    const size_t row = static_cast<size_t>(c->g.n_ox) * c->g.n_t;
-    for (const auto& cp : c->copies)
-        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(d_img + cp.first * row, d_img + cp.second * row,
-                                            row * sizeof(float), cudaMemcpyDeviceToDevice,
-                                            c->stream));
+    PSM_CUDA_TRY(c->st, copy_rows(c, d_img, c->stream));
     return PSM_OK;
 }
 
@@ -1550,6 +1560,7 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
                                         c->stream));
     bool staged = false;  // the next slab's new inlines are in the staging area
     auto fresh_of = [&](int k) { return (slabs[k].i1 - slabs[k].i0) - keep[k]; };
+    std::vector<char> direct(static_cast<size_t>(n), 0);  // image already on the host
     for (int32_t k = 0; k < n; ++k) {
         const psm_slab& sl = slabs[k];
         // a buffer that set_geometry had to grow was reallocated (its size changed), and
@@ -1564,9 +1575,16 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
         for (int i = 0; i < 4; ++i)
             if ((i == 0 || i == 3 || c->store != psm::kStoreF32) && bufs[i]->bytes != sizes[i])
                 same_bufs = false;
-        if (!(had && same_bufs && keep[k] > 0 && staged)) {  // the whole slab, uploaded now
-            if ((rc = psm_set_traces(c, traces + sl.i0 * trace))) return rc;
-            if ((rc = psm_set_vrms(c, vrms + sl.i0 * trace))) return rc;
+        if (!(had && same_bufs && keep[k] > 0 && staged)) {
+            // the whole slab from the host (the first one, or after a gap): psm_forward_host
+            // uploads it in inline blocks while the output inlines whose buffers are complete
+            // migrate, and returns the slab's image (it clears the error word first, so
+            // report what the slabs before it flagged)
+            if (k > 0 && (rc = read_device_error(c))) return rc;
+            if ((rc = psm_forward_host(c, traces + sl.i0 * trace, vrms + sl.i0 * trace,
+                                       image + sl.o0 * row)))
+                return rc;
+            direct[k] = 1;
         } else {
             const int shift = sl.i0 - slabs[k - 1].i0;  // inlines
             const int kp = keep[k];
@@ -1613,19 +1631,16 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
         }
         staged = false;
         PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_placed, c->stream));  // staging free again
-        // migrate slab k into image buffer k % 2
-        if (k == 0) PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
-        float* img = c->str_img[k & 1].as<float>();
-        FwdParams P = volume_params(c);
-        P.image = img;
-        PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
-                                       c->g.amp_correction != 0, c->variant, c->stream, c->store,
-                                       c->g.compensated != 0));
-        for (const auto& cp : c->copies)  // padded output inlines repeat an edge inline
-            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(img + cp.first * row, img + cp.second * row,
-                                                row * sizeof(float), cudaMemcpyDeviceToDevice,
-                                                c->stream));
-        PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_done[k & 1], c->stream));
+        if (!direct[k]) {  // migrate slab k into image buffer k % 2 (slab 0 came direct)
+            float* img = c->str_img[k & 1].as<float>();
+            FwdParams P = volume_params(c);
+            P.image = img;
+            PSM_CUDA_TRY(c->st, launch_fwd(P, static_cast<int>(c->jobs.size()),
+                                           c->g.amp_correction != 0, c->variant, c->stream,
+                                           c->store, c->g.compensated != 0));
+            PSM_CUDA_TRY(c->st, copy_rows(c, img, c->stream));  // padded inlines
+            PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_done[k & 1], c->stream));
+        }
         // while slab k migrates: stage the next slab's new inlines (once slab k's placement
         // has read the staging area) ...
         if (k + 1 < n && keep[k + 1] > 0 && fresh_of(k + 1) > 0) {
@@ -1646,7 +1661,7 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             staged = true;  // nothing new to stage
         }
         // ... and return slab k - 1's image
-        if (k > 0) {
+        if (k > 0 && !direct[k - 1]) {
             const psm_slab& pv = slabs[k - 1];
             PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, c->ev_done[(k - 1) & 1], 0));
             PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row,
@@ -1656,7 +1671,7 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
         }
     }
-    if (n > 0) {
+    if (n > 0 && !direct[n - 1]) {
         const psm_slab& pv = slabs[n - 1];
         PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row, c->str_img[(n - 1) & 1].p,
                                             (pv.o1 - pv.o0) * row * sizeof(float),

@@ -1225,6 +1225,21 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB)
                                                       L, it);
 }
 
+// Padded output inlines repeat the migrated edge inline (main.cpp:268-285): row copies[k].x of
+// the image gets row copies[k].y, every copy in one launch (a source row is never a
+// destination).
+__global__ void copy_rows_kernel(float* __restrict__ img, const int2* __restrict__ copies,
+                                 int n_copies, size_t row) {
+    const size_t total = static_cast<size_t>(n_copies) * row;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int k = static_cast<int>(i / row);
+        const size_t e = i - static_cast<size_t>(k) * row;
+        const int2 cp = copies[k];
+        img[static_cast<size_t>(cp.x) * row + e] = img[static_cast<size_t>(cp.y) * row + e];
+    }
+}
+
 // ----------------------------------------------------------------------------- term count
 
 // One block per (job, output crossline); threads stride over t.  out[job] += terms.
