@@ -309,10 +309,10 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int jobi = blockIdx.z;
+    const int jobi = blockIdx.y;  // grid (crossline tiles, jobs, time tiles), deepest first
     const Job job = P.jobs[jobi];
     const int x0 = blockIdx.x * kTX;
-    const int T0 = blockIdx.y * kTT;
+    const int T0 = static_cast<int>(gridDim.z - 1 - blockIdx.z) * kTT;
 
     float T2[kJ], F4[kJ], BB[kJ], MK[kJ];
     float gmax[2], gmin[2];

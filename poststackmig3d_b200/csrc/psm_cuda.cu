@@ -249,7 +249,8 @@ cudaError_t launch_grid(K, const FwdParams& P_in, int n_jobs, size_t smem, cudaS
         P.stage_cap = std::max(stage_cap_for(K::MINB, K::STORE), P.ns);
         smem = std::min(smem, fwd_smem(P, K::STORE));
     }
-    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, (P.n_t + TT - 1) / TT, n_jobs);
+    if (n_jobs > 65535) return cudaErrorInvalidValue;  // grid y
+    dim3 grid((P.n_ox + psm::kTX - 1) / psm::kTX, n_jobs, (P.n_t + TT - 1) / TT);
     dim3 block(32 * (psm::kTX + 1));
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaError_t e = cudaStreamIsCapturing(s, &cap);
@@ -1214,8 +1215,9 @@ int adjoint_dev(psm_ctx* c, const float* d_rows, float* d_out) {
     }
     if (smem > kMaxDynSmem)
         return c->st.fail(PSM_ERR_UNSUPPORTED, "n_t / aperture too large for the adjoint ring");
-    dim3 grid((c->g.n_ox + psm::kTX - 1) / psm::kTX, (c->g.n_t + psm::kTT - 1) / psm::kTT,
-              n_jobs);
+    if (n_jobs > 65535) return c->st.fail(PSM_ERR_UNSUPPORTED, "more than 65535 output inlines");
+    dim3 grid((c->g.n_ox + psm::kTX - 1) / psm::kTX, n_jobs,
+              (c->g.n_t + psm::kTT - 1) / psm::kTT);
     dim3 block(32 * (psm::kTX + 1));
     const bool amp = c->g.amp_correction != 0;
     cudaError_t e;
@@ -1560,7 +1562,6 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
                                         c->stream));
     bool staged = false;  // the next slab's new inlines are in the staging area
     auto fresh_of = [&](int k) { return (slabs[k].i1 - slabs[k].i0) - keep[k]; };
-    std::vector<char> direct(static_cast<size_t>(n), 0);  // image already on the host
     for (int32_t k = 0; k < n; ++k) {
         const psm_slab& sl = slabs[k];
         // a buffer that set_geometry had to grow was reallocated (its size changed), and
@@ -1575,16 +1576,9 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
         for (int i = 0; i < 4; ++i)
             if ((i == 0 || i == 3 || c->store != psm::kStoreF32) && bufs[i]->bytes != sizes[i])
                 same_bufs = false;
-        if (!(had && same_bufs && keep[k] > 0 && staged)) {
-            // the whole slab from the host (the first one, or after a gap): psm_forward_host
-            // uploads it in inline blocks while the output inlines whose buffers are complete
-            // migrate, and returns the slab's image (it clears the error word first, so
-            // report what the slabs before it flagged)
-            if (k > 0 && (rc = read_device_error(c))) return rc;
-            if ((rc = psm_forward_host(c, traces + sl.i0 * trace, vrms + sl.i0 * trace,
-                                       image + sl.o0 * row)))
-                return rc;
-            direct[k] = 1;
+        if (!(had && same_bufs && keep[k] > 0 && staged)) {  // the whole slab, uploaded now
+            if ((rc = psm_set_traces(c, traces + sl.i0 * trace))) return rc;
+            if ((rc = psm_set_vrms(c, vrms + sl.i0 * trace))) return rc;
         } else {
             const int shift = sl.i0 - slabs[k - 1].i0;  // inlines
             const int kp = keep[k];
@@ -1631,7 +1625,8 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
         }
         staged = false;
         PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_placed, c->stream));  // staging free again
-        if (!direct[k]) {  // migrate slab k into image buffer k % 2 (slab 0 came direct)
+        {  // migrate slab k into image buffer k % 2
+            if (k == 0) PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
             float* img = c->str_img[k & 1].as<float>();
             FwdParams P = volume_params(c);
             P.image = img;
@@ -1661,7 +1656,7 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             staged = true;  // nothing new to stage
         }
         // ... and return slab k - 1's image
-        if (k > 0 && !direct[k - 1]) {
+        if (k > 0) {
             const psm_slab& pv = slabs[k - 1];
             PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, c->ev_done[(k - 1) & 1], 0));
             PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row,
@@ -1671,7 +1666,7 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
         }
     }
-    if (n > 0 && !direct[n - 1]) {
+    if (n > 0) {
         const psm_slab& pv = slabs[n - 1];
         PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row, c->str_img[(n - 1) & 1].p,
                                             (pv.o1 - pv.o0) * row * sizeof(float),

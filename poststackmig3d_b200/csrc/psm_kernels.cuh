@@ -1138,7 +1138,15 @@ __device__ __forceinline__ void ring_init(unsigned char* smem_raw, const SmemLay
     fence_barrier_init();
 }
 
-// One tile per CTA: grid (crossline tiles, time tiles, jobs).
+// One tile per CTA: grid (crossline tiles, jobs, time tiles).  The time tile is the slowest
+// dimension, deepest first: the block scheduler starts CTAs in grid order, and a deep tile
+// holds several times the terms of a shallow one (the aperture grows with t0), so the light
+// tiles come last and the launch's tail is short.
+template <int J>
+__device__ __forceinline__ int grid_T0() {
+    return static_cast<int>(gridDim.z - 1 - blockIdx.z) * 32 * J;
+}
+
 template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
           bool PAIRS = false>
 __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams P) {
@@ -1147,7 +1155,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
     if (threadIdx.x == 0) ring_init(smem_raw, L);  // ordered by the tile's first barrier
     uint32_t it = 0;
     fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
-        P, P.jobs[blockIdx.z], blockIdx.x * kTX, blockIdx.y * 32 * J, smem_raw, L, it);
+        P, P.jobs[blockIdx.y], blockIdx.x * kTX, grid_T0<J>(), smem_raw, L, it);
 }
 
 // The same with 3 CTAs per SM (27 warps): registers are held to 72 per thread and the launcher
@@ -1160,7 +1168,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdPara
     if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
     fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
-        P, P.jobs[blockIdx.z], blockIdx.x * kTX, blockIdx.y * 32 * J, smem_raw, L, it);
+        P, P.jobs[blockIdx.y], blockIdx.x * kTX, grid_T0<J>(), smem_raw, L, it);
 }
 
 
