@@ -253,7 +253,8 @@ typedef enum {
     PSM_FWD_SCALAR_G4_O3 = 10,
     PSM_FWD_PAIRS_O3 = 11, /* mirrored inlines c - d, c + d staged as pairs, 3 CTAs per SM */
     PSM_FWD_PAIRS = 12,
-    PSM_FWD_N_VARIANTS = 13
+    PSM_FWD_PAIRS_J4_O4 = 13, /* pairs, tiles of 128 samples, 4 CTAs per SM (56 registers) */
+    PSM_FWD_N_VARIANTS = 14
 } psm_fwd_variant;
 int psm_set_variant(psm_ctx *ctx, int variant);
 int psm_get_variant(psm_ctx *ctx, int *variant);

@@ -142,16 +142,18 @@ struct KernelTag {
     static constexpr int GB = GB_, J = J_, STORE = STORE_, MINB = MINB_;
 };
 
-// Samples per stage of the kernel built for 3 CTAs per SM (32 KB), so that its shared memory
-// fits the SM three times.
+// Samples per stage of the kernel built for 3 CTAs per SM (32 KB) or 4 (20 KB), so that its
+// shared memory fits the SM three or four times.
 inline int stage_cap_for(int minb, int store) {
-    const int bytes = minb == 3 ? 32768 : 8 * psm::kStageCapMin;
+    const int bytes = minb == 4 ? 20480 : minb == 3 ? 32768 : 8 * psm::kStageCapMin;
     return bytes / psm::store_bytes(store);
 }
 
 template <class K>
 auto grid_kernel() {
-    if constexpr (K::MINB == 3)
+    if constexpr (K::MINB == 4)
+        return psm::fwd_kernel_o4<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
+    else if constexpr (K::MINB == 3)
         return psm::fwd_kernel_o3<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
     else
         return psm::fwd_kernel<K::AMP, K::PACKED, K::GB, K::J, K::STORE, K::KAHAN, K::PAIRS>;
@@ -200,6 +202,8 @@ cudaError_t with_kernel_amp(int variant, int store, bool kahan, F&& f) {
                 case PSM_FWD_PAIRS_O3:
                     return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 3, true>{});
                 case PSM_FWD_PAIRS: return f(KernelTag<AMP, true, 4, 8, kStoreF32, false, 2, true>{});
+                case PSM_FWD_PAIRS_J4_O4:
+                    return f(KernelTag<AMP, true, 4, 4, kStoreF32, false, 4, true>{});
 
 
                 default: return cudaErrorInvalidValue;

@@ -1171,6 +1171,18 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdPara
         P, P.jobs[blockIdx.y], blockIdx.x * kTX, grid_T0<J>(), smem_raw, L, it);
 }
 
+// The same with 4 CTAs per SM (36 warps): 56 registers per thread and 20 KB stages; for
+// tiles of 128 samples (J = 4), whose per-lane state is half that of J = 8.
+template <bool AMP, bool PACKED, int GB, int J, int STORE = kStoreF32, bool KAHAN = false,
+          bool PAIRS = false>
+__global__ void __launch_bounds__(32 * (kTX + 1), 4) fwd_kernel_o4(const FwdParams P) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
+    if (threadIdx.x == 0) ring_init(smem_raw, L);
+    uint32_t it = 0;
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
+        P, P.jobs[blockIdx.y], blockIdx.x * kTX, grid_T0<J>(), smem_raw, L, it);
+}
 
 // Parameters of every problem of a batched launch, passed by value: they live in the
 // kernel-parameter constant bank, whose loads are cached and uniform across the CTA.

@@ -439,7 +439,8 @@ class Migrator:
 
     VARIANTS = {1: "scalar/g2", 2: "scalar/g4", 3: "packed/g2", 4: "packed/g4",
                 5: "packed/g4/j16", 6: "scalar/g4/j16", 7: "packed/g8", 8: "scalar/g8",
-                9: "packed/g4/o3", 10: "scalar/g4/o3", 11: "pairs/o3", 12: "pairs"}
+                9: "packed/g4/o3", 10: "scalar/g4/o3", 11: "pairs/o3", 12: "pairs",
+                13: "pairs/j4/o4"}
 
     def set_variant(self, variant: int) -> None:
         check(self._L.psm_set_variant(self._ctx, int(variant)), self._err)
