@@ -85,7 +85,7 @@ def test_inline_dropin_matches_oracle():
         assert rms <= REL_RMS_TOL and mx <= MAX_REL_TOL, (cur_il, xs, rms, mx)
 
 
-PAIRED = {11, 12}  # variants that add mirrored traces' samples before the weight
+PAIRED = {11, 12, 13}  # variants that add mirrored traces' samples before the weight
 
 
 @pytest.mark.parametrize("seed,pad_il,angle", [(31, 0, 50.0), (32, 3, 35.0)])
