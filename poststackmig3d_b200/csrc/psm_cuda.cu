@@ -1715,9 +1715,9 @@ struct psm_batch {
     int max_ns = 0;  // longest trace stride over the problems
     int grid = 1;  // persistent CTAs
     int order = PSM_ORDER_DEPTH_FIRST;
-    // tile lists [time tile 256 / 512 samples (8 / 16 blocks a lane)][order]
-    int n_items[4] = {0, 0, 0, 0};
-    DevBuf items[4];
+    // tile lists [time tile 128 / 256 / 512 samples (4 / 8 / 16 blocks a lane)][order]
+    int n_items[6] = {0, 0, 0, 0, 0, 0};
+    DevBuf items[6];
     std::unique_ptr<psm::BatchParams> params;  // every problem's FwdParams (kernel argument)
     DevBuf counter, il_pos;
     cudaGraphExec_t exec = nullptr;
@@ -1729,6 +1729,11 @@ struct psm_batch {
 };
 
 namespace {
+
+// The tile list of a kernel whose time tile is 32 J samples, in the given order.
+constexpr int item_list(int J, int order) { return 2 * (J == 4 ? 0 : (J == 8 ? 1 : 2)) + order; }
+static_assert(item_list(4, 1) == 1 && item_list(8, 0) == 2 && item_list(16, 1) == 5,
+              "tile list index");
 
 // Shared-memory attribute and persistent grid (resident CTAs on every SM) of the batch
 // kernel K; done before a stream capture, so the graph holds only the launch.
@@ -1755,7 +1760,7 @@ cudaError_t prepare_persistent(K, psm_batch& b) {
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, b.ctx->device);
     if (e != cudaSuccess) return e;
-    const int w = (K::J == 16 ? 2 : 0) + b.order;
+    const int w = item_list(K::J, b.order);
     b.grid = std::max(1, std::min(b.n_items[w], n_sm * std::max(per_sm, 1)));
     return cudaSuccess;
 }
@@ -1766,7 +1771,7 @@ cudaError_t launch_persistent(K, const psm_batch& b, cudaStream_t s) {
                                        K::PAIRS, K::MINB>;
     const int cap = persistent_stage_cap<K>(b);
     const size_t smem = psm::smem_layout(b.max_inl, cap, psm::store_bytes(K::STORE)).total;
-    const int w = (K::J == 16 ? 2 : 0) + b.order;
+    const int w = item_list(K::J, b.order);
     const psm::BatchParams* params = b.params.get();
     std::unique_ptr<psm::BatchParams> small;
     if constexpr (K::MINB > 2) {  // every problem stages into the smaller stages
@@ -1799,7 +1804,7 @@ cudaError_t launch_items(K, const psm_batch& b, cudaStream_t s) {
                                        K::PAIRS, K::MINB>;
     const int cap = persistent_stage_cap<K>(b);
     const size_t smem = psm::smem_layout(b.max_inl, cap, psm::store_bytes(K::STORE)).total;
-    const int w = (K::J == 16 ? 2 : 0) + b.order;
+    const int w = item_list(K::J, b.order);
     if (b.n_items[w] <= 0) return cudaSuccess;
     const psm::BatchParams* params = b.params.get();
     std::unique_ptr<psm::BatchParams> small;
@@ -2066,15 +2071,15 @@ int psm_batch_create(psm_ctx* c, const psm_problem* problems, int n, psm_batch**
         if (vk != PSM_VRMS_CUBE) P.vs_x = P.vs_row = 0;  // one Vrms trace for every point
         b->params->p[i] = P;
     }
-    // tile lists, for 256- and 512-sample time tiles, in two orders:
+    // tile lists, for 128-, 256- and 512-sample time tiles, in two orders:
     //  * depth first: deepest time tiles first (the aperture, and so the work, grows with
     //    t0), then output inline, crossline tile and problem, so panels over one cube take
     //    the same tile one after another and the long tiles start early;
     //  * problem after problem, each in the grid kernel's order (crossline tile fastest,
     //    then time tile, then output inline).
     PSM_CUDA_TRY(c->st, b->counter.ensure(sizeof(int)));
-    for (int w = 0; w < 4; ++w) {
-        const int TT = 32 * (w >= 2 ? 16 : 8);
+    for (int w = 0; w < 6; ++w) {
+        const int TT = 32 * (4 << (w / 2));
         std::vector<psm::BatchItem> items;
         for (int i = 0; i < n; ++i) {
             const BatchProblem& p = b->probs[i];

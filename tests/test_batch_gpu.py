@@ -52,7 +52,7 @@ def _single(W, g, variant=0):
     return img, n
 
 
-@pytest.mark.parametrize("variant", [0, 5, 1])
+@pytest.mark.parametrize("variant", [0, 5, 1, 11, 13])
 @pytest.mark.parametrize("mode,order", [(Batch.PERSISTENT, Batch.DEPTH_FIRST),
                                         (Batch.PERSISTENT, Batch.PROBLEM_ORDER),
                                         (Batch.PER_PROBLEM, Batch.DEPTH_FIRST),
