@@ -627,10 +627,14 @@ def run_lsm(args):
     clk.start()
     time.sleep(0.25)
     # the call uploads the data, runs the initial forward (s = M r) and downloads the image
-    # around its iterations: time it with 0 iterations too, and report the difference
-    t = time.perf_counter()
+    # around its iterations: time it with 0 iterations too (the faster of two calls, after
+    # an untimed one), and report the difference
     m.lsm_cg(d, 0)
-    secs0 = time.perf_counter() - t
+    secs0 = float("inf")
+    for _ in range(2):
+        t = time.perf_counter()
+        m.lsm_cg(d, 0)
+        secs0 = min(secs0, time.perf_counter() - t)
     t = time.perf_counter()
     img, hist = m.lsm_cg(d, iters)
     secs = time.perf_counter() - t
@@ -638,8 +642,10 @@ def run_lsm(args):
     m.close()
     line = {"metric": "least-squares migration, 10 CG iterations",
             "value": (secs - secs0) / iters * 1e3,
+            "unit": "ms/iteration", "n_gpus": 1, "steps": iters, "warmup": 1,
+            "ms_per_step": (secs - secs0) / iters * 1e3,
             "call_ms": secs * 1e3, "call_ms_0_iterations": secs0 * 1e3,
-            "unit": "ms/iteration", "higher_is_better": False,
+            "higher_is_better": False,
             "config": {"workload": "config5: 201x201 traces x 1001 samples, V 2000 m/s, "
                                    "30 deg, 2% Laplace reflectivity, 5% noise",
                        "iterations": iters},

@@ -145,8 +145,7 @@ struct KernelTag {
 // Samples per stage of the kernel built for 3 CTAs per SM (32 KB) or 4 (20 KB), so that its
 // shared memory fits the SM three or four times.
 inline int stage_cap_for(int minb, int store) {
-    const int bytes = minb == 4 ? 20480 : minb == 3 ? 32768 : 8 * psm::kStageCapMin;
-    return bytes / psm::store_bytes(store);
+    return psm::stage_bytes_for(minb) / psm::store_bytes(store);
 }
 
 template <class K>

@@ -41,6 +41,14 @@ constexpr int kStages = 2;      // TMA ring depth
 constexpr int kMaxG = 32;       // traces per ring stage
 static_assert(kTX % 4 == 0, "per-slot r^2 rows are stored as float4");
 constexpr int kStageCapMin = 6144;          // samples (8 B each) per ring stage, at least
+// Bytes of one ring stage of a forward kernel built for minb CTAs per SM, and the offset of
+// a mirrored pair's second window from its first: half a stage, a compile-time constant, so
+// that the consumers read the second trace through the first trace's address plus an
+// immediate offset.
+__host__ __device__ constexpr int stage_bytes_for(int minb) {
+    return minb == 4 ? 20480 : minb == 3 ? 32768 : 8 * kStageCapMin;
+}
+__host__ __device__ constexpr int pair_off_bytes(int minb) { return stage_bytes_for(minb) / 2; }
 // mbarrier waits end after FwdParams::wait_us of %globaltimer time (kDefaultWaitUs when 0),
 // or after kWaitPollCap polls, whichever comes first
 constexpr unsigned kDefaultWaitUs = 4000000u;
@@ -546,7 +554,8 @@ __device__ __forceinline__ void term_pair(const unsigned char* sbase, float r2, 
 // crossline): the same travel times, sample indices, fractions and weights.  Interpolation is
 // linear in the samples, so the NT staged (d[lo], d[lo+1] - d[lo]) pairs are added first and
 // interpolated once; each trace's window has its own base.
-template <bool AMP, bool MASK, int NT>
+// POFF > 0: trace n's window lies n POFF bytes after the first's (base[n] unused).
+template <bool AMP, bool MASK, int NT, int POFF>
 __device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
                                            const uint32_t (&base)[2], const Win& w,
                                            const float2& T2, const float2& F4, const float2& BB,
@@ -561,12 +570,19 @@ __device__ __forceinline__ void term_multi(const unsigned char* sbase, float r2,
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
     const uint32_t o0 = __float_as_uint(mm.x) << 3, o1 = __float_as_uint(mm.y) << 3;
-    float2 a0 = *reinterpret_cast<const float2*>(sbase + (base[0] + o0));
-    float2 a1 = *reinterpret_cast<const float2*>(sbase + (base[0] + o1));
+    const unsigned char* p0 = sbase + (base[0] + o0);
+    const unsigned char* p1 = sbase + (base[0] + o1);
+    float2 a0 = *reinterpret_cast<const float2*>(p0);
+    float2 a1 = *reinterpret_cast<const float2*>(p1);
 #pragma unroll
     for (int n = 1; n < NT; ++n) {
-        a0 = add2(a0, *reinterpret_cast<const float2*>(sbase + (base[n] + o0)));
-        a1 = add2(a1, *reinterpret_cast<const float2*>(sbase + (base[n] + o1)));
+        if (POFF > 0) {
+            a0 = add2(a0, *reinterpret_cast<const float2*>(p0 + n * POFF));
+            a1 = add2(a1, *reinterpret_cast<const float2*>(p1 + n * POFF));
+        } else {
+            a0 = add2(a0, *reinterpret_cast<const float2*>(sbase + (base[n] + o0)));
+            a1 = add2(a1, *reinterpret_cast<const float2*>(sbase + (base[n] + o1)));
+        }
     }
     float2 v = make_float2(fmaf(fr.x, a0.y, a0.x), fmaf(fr.y, a1.y, a1.x));
     if (MASK) {
@@ -623,7 +639,7 @@ __device__ __forceinline__ void term_pair16(const unsigned char* sbase, float r2
 
 // Block pair of a mirrored pair of staged traces in 16-bit storage: as term_pair2, each trace's
 // interpolated value scaled by its own trace scale before the two are added.
-template <bool AMP, bool MASK, int STORE>
+template <bool AMP, bool MASK, int STORE, int POFF>
 __device__ __forceinline__ void term_pair2_16(const unsigned char* sbase, float r2,
                                               uint32_t base2a, uint32_t base2b, const Win& w,
                                               float sca, float scb, const float2& T2,
@@ -638,10 +654,14 @@ __device__ __forceinline__ void term_pair2_16(const unsigned char* sbase, float 
     const float2 mm = add2_rm(s, M);                         // 2^23 + floor(s)
     const float2 fr = sub2(s, sub2(mm, M));                  // frac
     const uint32_t o0 = __float_as_uint(mm.x) << 2, o1 = __float_as_uint(mm.y) << 2;
-    const float2 a0 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2a + o0)));
-    const float2 a1 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2a + o1)));
-    const float2 b0 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2b + o0)));
-    const float2 b1 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(sbase + (base2b + o1)));
+    const unsigned char* pa0 = sbase + (base2a + o0);
+    const unsigned char* pa1 = sbase + (base2a + o1);
+    const unsigned char* pb0 = POFF > 0 ? pa0 + POFF : sbase + (base2b + o0);
+    const unsigned char* pb1 = POFF > 0 ? pa1 + POFF : sbase + (base2b + o1);
+    const float2 a0 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(pa0));
+    const float2 a1 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(pa1));
+    const float2 b0 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(pb0));
+    const float2 b1 = unpack16<STORE>(*reinterpret_cast<const uint32_t*>(pb1));
     const float2 la = make_float2(a0.x, a1.x), lb = make_float2(b0.x, b1.x);
     const float2 va = fma2(fr, sub2(make_float2(a0.y, a1.y), la), la);  // simdInterpolate
     const float2 vb = fma2(fr, sub2(make_float2(b0.y, b1.y), lb), lb);
@@ -658,17 +678,17 @@ __device__ __forceinline__ void term_pair2_16(const unsigned char* sbase, float 
 
 // One block pair of a staged slot: a single trace (fp32 or 16-bit storage), or NT traces
 // sharing r^2 (mirrored inlines; 16-bit storage: NT = 2 only).
-template <bool AMP, bool MASK, bool PACKED, int STORE, int NT>
+template <bool AMP, bool MASK, bool PACKED, int STORE, int NT, int POFF>
 __device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2,
                                           const uint32_t (&base)[2], const Win& w, float sc,
                                           float scb, const float2& T2, const float2& F4,
                                           const float2& BB, float2& ACC) {
     static_assert(NT == 1 || NT == 2, "traces per slot");
     if (NT > 1 && STORE == kStoreF32)
-        term_multi<AMP, MASK, NT>(sbase, r2, base, w, T2, F4, BB, ACC);
+        term_multi<AMP, MASK, NT, POFF>(sbase, r2, base, w, T2, F4, BB, ACC);
     else if (NT > 1)
-        term_pair2_16<AMP, MASK, STORE>(sbase, r2, base[0], base[1], w, sc, scb, T2, F4, BB,
-                                        ACC);
+        term_pair2_16<AMP, MASK, STORE, POFF>(sbase, r2, base[0], base[1], w, sc, scb, T2, F4,
+                                              BB, ACC);
     else if (STORE == kStoreF32)
         term_pair<AMP, MASK, PACKED>(sbase, r2, base[0], w, T2, F4, BB, ACC);
     else
@@ -677,7 +697,7 @@ __device__ __forceinline__ void eval_pair(const unsigned char* sbase, float r2,
 
 // One staged slot for one consumer warp: every block pair of the lane where some lane of its
 // group passes, without masks where every lane of the group (or of the tile) passes.
-template <bool AMP, bool PACKED, int GB, int J, int STORE, int NT>
+template <bool AMP, bool PACKED, int GB, int J, int STORE, int NT, int POFF>
 __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
                                            const uint32_t (&base)[2], const Win& w,
                                            float sc, float scb,
@@ -690,8 +710,8 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
     if (r2 <= gminall) {  // interior trace: every term of the tile passes
 #pragma unroll
         for (int p = 0; p < J / 2; ++p)
-            eval_pair<AMP, false, PACKED, STORE, NT>(sbase, r2, base, w, sc, scb,
-                                                      T2[p], F4[p], BB[p], SUM[p]);
+            eval_pair<AMP, false, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
+                                                            T2[p], F4[p], BB[p], SUM[p]);
         return;
     }
 #pragma unroll
@@ -700,13 +720,14 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
             if (r2 <= gmin[gr]) {  // every lane of the group passes
 #pragma unroll
                 for (int p = PG * gr; p < PG * (gr + 1); ++p)
-                    eval_pair<AMP, false, PACKED, STORE, NT>(sbase, r2, base, w, sc, scb,
-                                                             T2[p], F4[p], BB[p], SUM[p]);
+                    eval_pair<AMP, false, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
+                                                                   T2[p], F4[p], BB[p], SUM[p]);
             } else {
 #pragma unroll
                 for (int p = PG * gr; p < PG * (gr + 1); ++p)
-                    eval_pair<AMP, true, PACKED, STORE, NT>(sbase, r2, base, w, sc,
-                                                             scb, T2[p], F4[p], BB[p], SUM[p]);
+                    eval_pair<AMP, true, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc,
+                                                                   scb, T2[p], F4[p], BB[p],
+                                                                   SUM[p]);
             }
         }
     }
@@ -731,7 +752,10 @@ struct BatchItem {
     int prob, job, x0, T0;
 };
 
-template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false>
+// POFF (PAIRS): bytes from a mirrored pair's first window to its second (pair_off_bytes of
+// the kernel's CTAs per SM).
+template <bool AMP, bool PACKED, int GB, int J, int STORE, bool KAHAN, bool PAIRS = false,
+          int POFF = 0>
 __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int x0, int T0,
                                          unsigned char* smem_raw, const SmemLayout& L,
                                          uint32_t& it) {
@@ -739,6 +763,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
     static_assert(J % GB == 0, "whole skip groups per lane");
     static_assert(STORE == kStoreF32 || PACKED, "16-bit storage uses packed arithmetic");
     static_assert(!PAIRS || PACKED, "mirrored pairs use packed arithmetic");
+    static_assert(!PAIRS || (POFF > 0 && POFF % 16 == 0), "pair windows 16-byte aligned");
     constexpr int NG = J / GB;   // skip groups per lane
     constexpr int EB = store_bytes(STORE);
     // bits(2^23) << log2(EB), modulo 2^32 (see the producer)
@@ -863,12 +888,17 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         // rows of the trace list: the buffer inlines, or (PAIRS) the mirror distances d from the
         // centre inline pc, row d holding inlines pc - d and pc + d, whose traces at one
         // crossline have the same r^2 to every output point
-        int pc = -1;  // pairs need two whole windows in one stage (a window is at most ns)
-        if (PAIRS && P.pairable && 2 * P.ns <= P.stage_cap && n_inl > 0) {
+        // pairs: a pair's second window lies POFF bytes after its first, so the first windows
+        // of all slots fill the stage's first POFF bytes, where a whole window (at most ns
+        // samples) must fit
+        int pc = -1;
+        if (PAIRS && P.pairable && P.ns * EB <= POFF && P.stage_cap * EB >= 2 * POFF &&
+            n_inl > 0) {
             const int c = job.pos - __ldg(P.il_pos + job.i0);
             if (c >= 0 && c < n_inl) pc = c;
         }
         const int n_rows = pc >= 0 ? max(pc, n_inl - 1 - pc) + 1 : n_inl;
+        const int cap = pc >= 0 ? POFF / EB : P.stage_cap;  // samples of first windows a stage
         int total = 0;
         if (S.any && xa <= xb) {
             // row table: crossline range and running slot count per row
@@ -907,7 +937,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
         int f = 0;
         while (f < total && alive) {
             const int idx = f + lane;
-            int ws = 0, size = 0, kc = 0, row = 0, rowb = -1, slot_size = 0;
+            int ws = 0, size = 0, kc = 0, row = 0, rowb = -1, slot_size = 0, tx_size = 0;
             float dx2 = 0.0f, sc = 1.0f, scb = 1.0f;
             if (idx < total) {
                 // row of flat slot idx: the last n with inl_pre[n] <= idx
@@ -930,7 +960,8 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     sc = __ldg(P.scales + static_cast<size_t>(row) * P.n_cx + kc);
                     if (rowb >= 0) scb = __ldg(P.scales + static_cast<size_t>(rowb) * P.n_cx + kc);
                 }
-                slot_size = rowb >= 0 ? 2 * size : size;  // a pair's windows are the same
+                slot_size = size;                        // samples of the first region
+                tx_size = rowb >= 0 ? 2 * size : size;   // samples copied (a pair: both)
             }
             // inclusive prefix sum of slot sizes; take the lanes that fit one stage
             int cum = slot_size;
@@ -939,7 +970,7 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                 const int v = __shfl_up_sync(0xffffffffu, cum, o);
                 if (lane >= o) cum += v;
             }
-            const bool take = cum <= P.stage_cap;
+            const bool take = cum <= cap;
             const unsigned takemask = __ballot_sync(0xffffffffu, take);
             const int consumed = __popc(takemask);
             const unsigned nzmask = __ballot_sync(0xffffffffu, take && size > 0);
@@ -955,7 +986,9 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                 // test-only: the tile's first stage is never filled nor arrived on
                 const bool stall = (P.fault & kFaultStallProducer) && it == it_begin;
                 StageMeta& m = meta[stage];
-                const int tot = __shfl_sync(0xffffffffu, take ? cum : 0, consumed - 1);
+                const int tot = __reduce_add_sync(0xffffffffu, take ? tx_size : 0);  // samples
+                const uint32_t boff =  // a pair's second window from its first (bytes)
+                    POFF > 0 ? static_cast<uint32_t>(POFF) : static_cast<uint32_t>(size) * EB;
                 const uint32_t dst_rel =
                     L.stage +
                     (static_cast<uint32_t>(stage) * P.stage_cap + (cum - slot_size)) * EB;
@@ -965,10 +998,10 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                     // consumers find sample n of the window at byte
                     // base2 + (bits(2^23 + n) << log2(EB)) from the shared-memory base (32-bit
                     // wrap-around): base2 = dst_rel - EB ws - (0x4B000000 << log2(EB)); a
-                    // pair's second window follows its first
+                    // pair's second window lies boff bytes after its first
                     m.m[slot] = make_int4(static_cast<int>(dst_rel - EB * ws - MAGIC),
                                           __float_as_int(static_cast<float>(ws)),
-                                          static_cast<int>(dst_rel + EB * size - EB * ws - MAGIC),
+                                          static_cast<int>(dst_rel + boff - EB * ws - MAGIC),
                                           rowb >= 0 ? 1 : 0);
                     m.sc[slot] = sc;
                     m.wend[slot] = static_cast<float>(ws + size);
@@ -998,13 +1031,13 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
                                           ? static_cast<const void*>(P.pairs + off)
                                           : static_cast<const void*>(P.words + off);
                     tma_load_1d(dst, src, static_cast<uint32_t>(size) * EB, &full[stage]);
-                    if (rowb >= 0) {  // the mirrored trace's window right after
+                    if (rowb >= 0) {  // the mirrored trace's window, boff bytes on
                         const size_t offb = (static_cast<size_t>(rowb) * P.n_cx + kc) * P.ns + ws;
                         const void* srcb = STORE == kStoreF32
                                                ? static_cast<const void*>(P.pairs + offb)
                                                : static_cast<const void*>(P.words + offb);
-                        tma_load_1d(dst + static_cast<uint32_t>(size) * EB, srcb,
-                                    static_cast<uint32_t>(size) * EB, &full[stage]);
+                        tma_load_1d(dst + boff, srcb, static_cast<uint32_t>(size) * EB,
+                                    &full[stage]);
                     }
                 }
                 ++it;
@@ -1076,13 +1109,14 @@ __device__ __forceinline__ bool fwd_tile(const FwdParams& P, const Job job, int 
             const float sc = STORE == kStoreF32 ? 1.0f : m.sc[g];
             if (PAIRS && md.w) {
                 base[1] = static_cast<uint32_t>(md.z);
-                visit_slot<AMP, PACKED, GB, J, STORE, 2>(
+                visit_slot<AMP, PACKED, GB, J, STORE, 2, POFF>(
                     smem_raw, r2, base, w, sc, STORE == kStoreF32 ? 1.0f : m.scb[g],
                     gminall, gmax, gmin, T2, F4, BB, SUM);
             } else {
                 base[1] = 0u;
-                visit_slot<AMP, PACKED, GB, J, STORE, 1>(smem_raw, r2, base, w, sc, 1.0f,
-                                                         gminall, gmax, gmin, T2, F4, BB, SUM);
+                visit_slot<AMP, PACKED, GB, J, STORE, 1, 0>(smem_raw, r2, base, w, sc, 1.0f,
+                                                            gminall, gmax, gmin, T2, F4, BB,
+                                                            SUM);
             }
         }
         if (KAHAN) {  // ACC += PART, compensated
@@ -1154,7 +1188,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 2) fwd_kernel(const FwdParams 
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);  // ordered by the tile's first barrier
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, PAIRS ? pair_off_bytes(2) : 0>(
         P, P.jobs[blockIdx.y], blockIdx.x * kTX, grid_T0<J>(), smem_raw, L, it);
 }
 
@@ -1167,7 +1201,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 3) fwd_kernel_o3(const FwdPara
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, PAIRS ? pair_off_bytes(3) : 0>(
         P, P.jobs[blockIdx.y], blockIdx.x * kTX, grid_T0<J>(), smem_raw, L, it);
 }
 
@@ -1180,7 +1214,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), 4) fwd_kernel_o4(const FwdPara
     const SmemLayout L = smem_layout(P.max_inl, P.stage_cap, store_bytes(STORE));
     if (threadIdx.x == 0) ring_init(smem_raw, L);
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, PAIRS ? pair_off_bytes(4) : 0>(
         P, P.jobs[blockIdx.y], blockIdx.x * kTX, grid_T0<J>(), smem_raw, L, it);
 }
 
@@ -1220,7 +1254,8 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB)
         __syncthreads();
         const BatchItem w = s_item;
         if (w.prob < 0) break;
-        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(
+        const bool ok = fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS,
+                                 PAIRS ? pair_off_bytes(MINB) : 0>(
             B.p[w.prob], s_job, w.x0, w.T0, smem_raw, L, it);
         // barrier: the tile's tables, statistics, s_item and s_job are reused next
         if (__syncthreads_or(!ok)) break;
@@ -1241,8 +1276,8 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB)
     const BatchItem w = items[blockIdx.x];
     const FwdParams& P = B.p[w.prob];
     uint32_t it = 0;
-    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS>(P, P.jobs[w.job], w.x0, w.T0, smem_raw,
-                                                      L, it);
+    fwd_tile<AMP, PACKED, GB, J, STORE, KAHAN, PAIRS, PAIRS ? pair_off_bytes(MINB) : 0>(
+        P, P.jobs[w.job], w.x0, w.T0, smem_raw, L, it);
 }
 
 // Padded output inlines repeat the migrated edge inline (main.cpp:268-285): row copies[k].x of

@@ -47,16 +47,16 @@ def test_dot_product(case):
     assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs)), (lhs, rhs)
 
 
-@pytest.mark.parametrize("accum", ["fixed", "f32"])
+ACCUMS = ["fixed", "f32"]
+
+
+@pytest.mark.parametrize("accum", ACCUMS)
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"seed{c['seed']}")
 def test_adjoint_matches_oracle(case, accum, monkeypatch):
-    """Both accumulations of the spray: fp32 shared-memory atomics into an fp32 cube (the
-    default) and 64-bit fixed-point windows into an FP64 data cube (PSM_ADJ_ACCUM=fixed, read
-    when the context is created)."""
-    if accum == "fixed":
-        monkeypatch.setenv("PSM_ADJ_ACCUM", "fixed")
-    else:
-        monkeypatch.delenv("PSM_ADJ_ACCUM", raising=False)
+    """Both accumulations of the spray (PSM_ADJ_ACCUM, read when the context is created):
+    fp32 shared-memory atomics into an fp32 cube (the default) and 64-bit fixed-point windows
+    into an FP64 data cube."""
+    monkeypatch.setenv("PSM_ADJ_ACCUM", accum)
     W, g, mig = _setup(case)
     rng = np.random.default_rng(8)
     im = rng.standard_normal((g.n_oi, g.n_ox, g.n_t)).astype(np.float32)
@@ -70,6 +70,26 @@ def test_adjoint_matches_oracle(case, accum, monkeypatch):
     # FP32 atomic accumulation of many contributions per data sample, against FP64 sums: the
     # FP32 parity bar of the forward operator
     assert rms <= 1e-4 and mx <= 1e-4, (rms, mx)
+
+
+@pytest.mark.parametrize("accum", ACCUMS)
+def test_adjoint_coherent_image(accum, monkeypatch):
+    """A constant image at a wide aperture (85 deg, no amplitude weight): the shares of a
+    window sample all have one sign, and near the aperture's edge (ds/dt0 = cos 85 deg) one
+    tile puts up to about 43 of its largest shares on one sample, where the fixed-point
+    windows' tile scale leaves the least headroom.  The sums must match the FP64 oracle."""
+    monkeypatch.setenv("PSM_ADJ_ACCUM", accum)
+    W, g, mig = _setup(dict(seed=55, n_il=12, n_xl=14, n_t=260, vel_kind="const",
+                            angle=85.0, amp=False))
+    im = np.ones((g.n_oi, g.n_ox, g.n_t), dtype=np.float32)
+    got = mig.adjoint(im)
+    mig.close()
+    ref = O.adjoint_volume(im.astype(np.float64), W.vrms_cube(), g.n_il, g.n_xl,
+                           g.out_center, g.pad_il, g.pad_xl, g.m_il, np.float32(g.dt_seconds),
+                           g.t0(), np.float32(g.tan2), g.d_il, g.d_xl, g.amp,
+                           flags=O.CONTRACT)
+    rms, mx = rel_err(got, ref)
+    assert rms <= 1e-5 and mx <= 1e-4, (rms, mx)
 
 
 def test_gradient_matches_finite_differences():
