@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -984,10 +985,15 @@ int psm_forward(psm_ctx* c, float* image) {
     return psm_get_image(c, image);
 }
 
-int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* image) {
-    if (!c || !traces || !vrms || !image) return PSM_ERR_ARG;
-    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
-    cudaSetDevice(c->device);
+}  // extern "C"
+
+namespace {
+
+// psm_forward_host's pipeline.  after_launches (may be empty) runs once every upload and
+// launch is enqueued, while the last waves migrate (psm_forward_streamed stages the next
+// slab's inlines there).
+int forward_waves(psm_ctx* c, const float* traces, const float* vrms, float* image,
+                  const std::function<int()>& after_launches) {
     const psm_geom& g = c->g;
     cudaStream_t s = c->stream;
     for (cudaStream_t* t : {&c->copy_stream, &c->d2h_stream, &c->aux_stream})
@@ -999,7 +1005,11 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
     // the first upload after which its buffer and Vrms row are resident.  Waves alternate
     // between two compute streams, so that one launch's tail of finishing CTAs overlaps the
     // next launch instead of idling SMs; the last wave is cut in two so that most of its rows
-    // stream back while the rest migrate.
+    // stream back while the rest migrate.  Each wave is enqueued right after the upload that
+    // completes its inputs: a copy from pageable memory returns only once the host has staged
+    // it, and the waves already enqueued migrate meanwhile.  The image rows' copies to the host
+    // are enqueued after every upload and launch: into pageable memory such a copy returns only
+    // once it is done, which would hold the next upload back until the wave has finished.
     const int n_blocks = std::min(g.n_il, 8);
     auto block_end = [&](int b) { return static_cast<int>(int64_t(b + 1) * g.n_il / n_blocks); };
     auto block_of = [&](int inl) {  // block holding inline inl
@@ -1077,6 +1087,14 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
     PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, ev_start, 0));
     PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->aux_stream, ev_start, 0));
     const size_t per_il = static_cast<size_t>(g.n_xl) * g.n_t;
+    const size_t row = static_cast<size_t>(g.n_ox) * g.n_t;
+    FwdParams P = volume_params(c);
+    bool aux_used = false;
+    size_t k = 0;  // next chunk
+    struct RowCopy {
+        size_t chunk, first, count;  // image rows [first, first + count) of chunk
+    };
+    std::vector<RowCopy> row_copies;
     for (int u = 0; u < n_units; ++u) {
         const int b = units[u].second;
         const int lo = b ? block_end(b - 1) : 0, hi = block_end(b);
@@ -1102,43 +1120,48 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
                                                 cudaMemcpyHostToDevice, cs));
         }
         PSM_CUDA_TRY(c->st, cudaEventRecord(ev[u], cs));
-    }
-    const size_t row = static_cast<size_t>(g.n_ox) * g.n_t;
-    FwdParams P = volume_params(c);
-    bool aux_used = false;
-    for (size_t k = 0; k < chunks.size(); ++k) {
-        cudaStream_t cs = (k % 2 == 0) ? s : c->aux_stream;
-        aux_used = aux_used || cs != s;
-        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(cs, ev[chunk_unit[k]], 0));
-        FwdParams Q = P;
-        Q.jobs = c->d_jobs_waves.as<Job>() + chunks[k].first;
-        PSM_CUDA_TRY(c->st, launch_fwd(Q, chunks[k].second, g.amp_correction != 0, c->variant,
-                                       cs, c->store, g.compensated != 0));
-        std::vector<int> out_rows;
-        for (int t = 0; t < chunks[k].second; ++t) {
-            const int r = order[chunks[k].first + t].row;
-            out_rows.push_back(r);
-            for (int d : dup[r]) {  // padded output inlines repeat the edge inline
-                PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.as<float>() + d * row,
-                                                    c->image.as<float>() + r * row,
-                                                    row * sizeof(float),
-                                                    cudaMemcpyDeviceToDevice, cs));
-                out_rows.push_back(d);
+        for (; k < chunks.size() && chunk_unit[k] == u; ++k) {  // the waves this upload frees
+            cudaStream_t ks = (k % 2 == 0) ? s : c->aux_stream;
+            aux_used = aux_used || ks != s;
+            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(ks, ev[u], 0));
+            FwdParams Q = P;
+            Q.jobs = c->d_jobs_waves.as<Job>() + chunks[k].first;
+            PSM_CUDA_TRY(c->st, launch_fwd(Q, chunks[k].second, g.amp_correction != 0,
+                                           c->variant, ks, c->store, g.compensated != 0));
+            std::vector<int> out_rows;
+            for (int t = 0; t < chunks[k].second; ++t) {
+                const int r = order[chunks[k].first + t].row;
+                out_rows.push_back(r);
+                for (int d : dup[r]) {  // padded output inlines repeat the edge inline
+                    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->image.as<float>() + d * row,
+                                                        c->image.as<float>() + r * row,
+                                                        row * sizeof(float),
+                                                        cudaMemcpyDeviceToDevice, ks));
+                    out_rows.push_back(d);
+                }
+            }
+            PSM_CUDA_TRY(c->st, cudaEventRecord(ev[n_units + k], ks));
+            std::sort(out_rows.begin(), out_rows.end());
+            for (size_t i = 0; i < out_rows.size();) {  // runs of consecutive rows
+                size_t e = i + 1;
+                while (e < out_rows.size() && out_rows[e] == out_rows[e - 1] + 1) ++e;
+                row_copies.push_back({k, static_cast<size_t>(out_rows[i]), e - i});
+                i = e;
             }
         }
-        cudaEvent_t done = ev[n_units + k];
-        PSM_CUDA_TRY(c->st, cudaEventRecord(done, cs));
-        PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, done, 0));
-        std::sort(out_rows.begin(), out_rows.end());
-        for (size_t i = 0; i < out_rows.size();) {  // runs of consecutive rows
-            size_t e = i + 1;
-            while (e < out_rows.size() && out_rows[e] == out_rows[e - 1] + 1) ++e;
-            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + out_rows[i] * row,
-                                                c->image.as<float>() + out_rows[i] * row,
-                                                (e - i) * row * sizeof(float),
-                                                cudaMemcpyDeviceToHost, c->d2h_stream));
-            i = e;
-        }
+    }
+    if (after_launches) {
+        const int r = after_launches();
+        if (r) return r;
+    }
+    for (size_t i = 0; i < row_copies.size(); ++i) {
+        const RowCopy& rc = row_copies[i];
+        if (i == 0 || row_copies[i - 1].chunk != rc.chunk)
+            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, ev[n_units + rc.chunk], 0));
+        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + rc.first * row,
+                                            c->image.as<float>() + rc.first * row,
+                                            rc.count * row * sizeof(float),
+                                            cudaMemcpyDeviceToHost, c->d2h_stream));
     }
     // the ctx stream's later work follows both compute streams and the uploads
     PSM_CUDA_TRY(c->st, cudaEventRecord(ev_aux, aux_used ? c->aux_stream : c->copy_stream));
@@ -1151,6 +1174,17 @@ int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* 
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
     c->have_traces = c->have_vrms = c->traces_readable = true;
     return read_device_error(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int psm_forward_host(psm_ctx* c, const float* traces, const float* vrms, float* image) {
+    if (!c || !traces || !vrms || !image) return PSM_ERR_ARG;
+    if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
+    cudaSetDevice(c->device);
+    return forward_waves(c, traces, vrms, image, {});
 }
 
 }  // extern "C"
@@ -1533,7 +1567,9 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
     // their buffers, and only the new inlines are uploaded and prepared.  The new inlines of
     // slab k + 1 go up into a staging area while slab k migrates, and slab k's image returns
     // to the host while slab k + 1 migrates (two image buffers in turn), so the copies hide
-    // behind the kernels.  The raw traces of the kept inlines are not kept: after this call
+    // behind the kernels.  A slab uploaded whole (the first) goes through psm_forward_host's
+    // pipeline: its output inlines migrate as soon as their inputs are up, and their image
+    // rows go straight to the host.  The raw traces of the kept inlines are not kept: after this call
     // the ctx holds the last slab's geometry and no readable traces.
     std::vector<psm_geom> loc(static_cast<size_t>(n));
     std::vector<std::vector<int32_t>> lcs(static_cast<size_t>(n));
@@ -1565,6 +1601,28 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
                                         c->stream));
     bool staged = false;  // the next slab's new inlines are in the staging area
     auto fresh_of = [&](int k) { return (slabs[k].i1 - slabs[k].i0) - keep[k]; };
+    // stage slab k's new inlines (once the previous placement has read the staging area)
+    auto stage = [&](int k) -> int {
+        if (k >= n || keep[k] <= 0) return PSM_OK;
+        if (fresh_of(k) > 0) {
+            const int kp = keep[k], fresh = fresh_of(k);
+            const size_t first = static_cast<size_t>(slabs[k].i0 + kp);
+            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, c->ev_placed, 0));
+            PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->str_tr.p, ns * sizeof(float),
+                                                  traces + first * trace,
+                                                  g->n_t * sizeof(float), g->n_t * sizeof(float),
+                                                  static_cast<size_t>(fresh) * per_il_tr,
+                                                  cudaMemcpyHostToDevice, c->copy_stream));
+            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->str_v.p, vrms + first * trace,
+                                                fresh * trace * sizeof(float),
+                                                cudaMemcpyHostToDevice, c->copy_stream));
+            PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_staged, c->copy_stream));
+        }
+        staged = true;  // (nothing new to stage when fresh_of(k) is 0)
+        return PSM_OK;
+    };
+    // slabs whose image rows went straight to the host (uploaded whole, in waves)
+    std::vector<char> direct(static_cast<size_t>(n), 0);
     for (int32_t k = 0; k < n; ++k) {
         const psm_slab& sl = slabs[k];
         // a buffer that set_geometry had to grow was reallocated (its size changed), and
@@ -1579,9 +1637,16 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
         for (int i = 0; i < 4; ++i)
             if ((i == 0 || i == 3 || c->store != psm::kStoreF32) && bufs[i]->bytes != sizes[i])
                 same_bufs = false;
-        if (!(had && same_bufs && keep[k] > 0 && staged)) {  // the whole slab, uploaded now
-            if ((rc = psm_set_traces(c, traces + sl.i0 * trace))) return rc;
-            if ((rc = psm_set_vrms(c, vrms + sl.i0 * trace))) return rc;
+        if (!(had && same_bufs && keep[k] > 0 && staged)) {
+            // the whole slab, uploaded in inline blocks: each output inline migrates once its
+            // inputs are up, and its image rows go straight to the host; the next slab's new
+            // inlines are staged while the last waves migrate
+            staged = false;
+            if (k > 0 && (rc = read_device_error(c))) return rc;  // (forward_waves clears it)
+            if ((rc = forward_waves(c, traces + sl.i0 * trace, vrms + sl.i0 * trace,
+                                    image + sl.o0 * row, [&] { return stage(k + 1); })))
+                return rc;
+            direct[k] = 1;
         } else {
             const int shift = sl.i0 - slabs[k - 1].i0;  // inlines
             const int kp = keep[k];
@@ -1626,9 +1691,9 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             c->have_traces = c->have_vrms = true;
             c->traces_readable = false;  // the raw cube rows were not moved
         }
-        staged = false;
-        PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_placed, c->stream));  // staging free again
-        {  // migrate slab k into image buffer k % 2
+        if (!direct[k]) {  // migrate slab k into image buffer k % 2
+            staged = false;
+            PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_placed, c->stream));  // staging free again
             if (k == 0) PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
             float* img = c->str_img[k & 1].as<float>();
             FwdParams P = volume_params(c);
@@ -1639,27 +1704,10 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             PSM_CUDA_TRY(c->st, copy_rows(c, img, c->stream));  // padded inlines
             PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_done[k & 1], c->stream));
         }
-        // while slab k migrates: stage the next slab's new inlines (once slab k's placement
-        // has read the staging area) ...
-        if (k + 1 < n && keep[k + 1] > 0 && fresh_of(k + 1) > 0) {
-            const int kp = keep[k + 1], fresh = fresh_of(k + 1);
-            const size_t first = static_cast<size_t>(slabs[k + 1].i0 + kp);
-            PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, c->ev_placed, 0));
-            PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->str_tr.p, ns * sizeof(float),
-                                                  traces + first * trace,
-                                                  g->n_t * sizeof(float), g->n_t * sizeof(float),
-                                                  static_cast<size_t>(fresh) * per_il_tr,
-                                                  cudaMemcpyHostToDevice, c->copy_stream));
-            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->str_v.p, vrms + first * trace,
-                                                fresh * trace * sizeof(float),
-                                                cudaMemcpyHostToDevice, c->copy_stream));
-            PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_staged, c->copy_stream));
-            staged = true;
-        } else if (k + 1 < n && keep[k + 1] > 0) {
-            staged = true;  // nothing new to stage
-        }
+        // while slab k migrates: stage the next slab's new inlines ...
+        if (!direct[k] && (rc = stage(k + 1))) return rc;
         // ... and return slab k - 1's image
-        if (k > 0) {
+        if (k > 0 && !direct[k - 1]) {
             const psm_slab& pv = slabs[k - 1];
             PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, c->ev_done[(k - 1) & 1], 0));
             PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row,
@@ -1669,7 +1717,7 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
         }
     }
-    if (n > 0) {
+    if (n > 0 && !direct[n - 1]) {
         const psm_slab& pv = slabs[n - 1];
         PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row, c->str_img[(n - 1) & 1].p,
                                             (pv.o1 - pv.o0) * row * sizeof(float),
@@ -2075,7 +2123,7 @@ int psm_batch_create(psm_ctx* c, const psm_problem* problems, int n, psm_batch**
     //    t0), then output inline, crossline tile and problem, so panels over one cube take
     //    the same tile one after another and the long tiles start early;
     //  * problem after problem, each in the grid kernel's order (crossline tile fastest,
-    //    then time tile, then output inline).
+    //    then output inline, then time tile, deepest first).
     PSM_CUDA_TRY(c->st, b->counter.ensure(sizeof(int)));
     for (int w = 0; w < 6; ++w) {
         const int TT = 32 * (4 << (w / 2));
@@ -2083,8 +2131,8 @@ int psm_batch_create(psm_ctx* c, const psm_problem* problems, int n, psm_batch**
         for (int i = 0; i < n; ++i) {
             const BatchProblem& p = b->probs[i];
             const psm_geom& g = p.src.geom;
-            for (int j = 0; j < static_cast<int>(p.jobs.size()); ++j)
-                for (int T0 = 0; T0 < g.n_t; T0 += TT)
+            for (int T0 = (g.n_t - 1) / TT * TT; T0 >= 0; T0 -= TT)
+                for (int j = 0; j < static_cast<int>(p.jobs.size()); ++j)
                     for (int x0 = 0; x0 < g.n_ox; x0 += psm::kTX) items.push_back({i, j, x0, T0});
         }
         if ((w & 1) == PSM_ORDER_DEPTH_FIRST)
