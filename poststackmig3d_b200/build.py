@@ -68,10 +68,10 @@ def build_cuda(force: bool = False, extra=()) -> str:
     todo = [(s, o) for s, o in zip(CUDA_SRC, objs)
             if force or _stale(o, [s] + CUDA_HDR)]
     with ThreadPoolExecutor(max_workers=len(CUDA_SRC)) as ex:
-        list(ex.map(lambda so: _run([NVCC, *ARCH, *NVCC_FLAGS, "-Xcompiler", "-fPIC",
+        list(ex.map(lambda so: _run([NVCC, *ARCH, *NVCC_FLAGS, "-Xcompiler", "-fPIC,-fopenmp",
                                      f"-I{INC}", *extra, "-c", "-o", so[1], so[0]]), todo))
     if force or todo or _stale(out, objs):
-        _run([NVCC, *ARCH, "-shared", "-o", out, *objs])
+        _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lgomp"])
     return out
 
 

@@ -1,5 +1,6 @@
 // libpsm_cuda.so: C ABI (include/psm.h) over the sm_100a migration kernels (psm_kernels.cuh).
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <atomic>
@@ -377,6 +378,53 @@ bool plan_jobs(const psm_geom& g, const int32_t* out_center, std::vector<Job>& j
 
 // ---------------------------------------------------------------------------- context
 
+namespace {
+
+// Pinned staging for copies between pageable host memory and the device.  The CUDA driver
+// copies pageable memory on one host thread through a small staging area of its own (about
+// 11 GB/s here); these copies go through kStagingSlots pinned buffers that host threads
+// (OpenMP) fill or drain in parallel, each buffer's device copy overlapping the host copy of
+// the next.  Pinned host memory is copied directly.  Allocated on first use, freed with the
+// context.
+constexpr size_t kStagingBytes = size_t(16) << 20;
+constexpr int kStagingSlots = 3;
+
+struct HostStaging {
+    void* buf[kStagingSlots] = {};
+    cudaEvent_t ev[kStagingSlots] = {};  // the last device copy that used each buffer
+    int next = 0;
+    int threads = 1;
+    bool ready = false;
+    cudaError_t init() {
+        if (ready) return cudaSuccess;
+        for (int i = 0; i < kStagingSlots; ++i) {
+            cudaError_t e = buf[i] ? cudaSuccess
+                                   : cudaHostAlloc(&buf[i], kStagingBytes, cudaHostAllocPortable);
+            if (e == cudaSuccess && !ev[i])
+                e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        // PSM_STAGING_THREADS host threads copy (default: half the processors, at most 8)
+        int t = std::max(1, std::min(8, omp_get_num_procs() / 2));
+        if (const char* v = std::getenv("PSM_STAGING_THREADS")) t = std::max(1, std::atoi(v));
+        threads = t;
+        ready = true;
+        return cudaSuccess;
+    }
+    void release() {
+        for (int i = 0; i < kStagingSlots; ++i) {
+            if (ev[i]) cudaEventSynchronize(ev[i]);
+            if (buf[i]) cudaFreeHost(buf[i]);
+            if (ev[i]) cudaEventDestroy(ev[i]);
+            buf[i] = nullptr;
+            ev[i] = nullptr;
+        }
+        ready = false;
+    }
+};
+
+}  // namespace
+
 struct psm_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -427,6 +475,7 @@ struct psm_ctx {
     // test-only failure injection (psm::kFault*), both read from the environment by psm_create
     unsigned wait_us = 0;
     int fault = 0;
+    HostStaging staging;  // pageable host copies
 };
 
 namespace {
@@ -486,6 +535,98 @@ FwdParams volume_params(psm_ctx* c) {
     P.stage_cap = stage_cap(c->ns, c->store);
     fill_consts(P, c->g.dt, c->g.d_il, c->g.d_xl, c->g.tan2_theta);
     return P;
+}
+
+// Host memory the CUDA driver copies through its own staging (not pinned or registered).
+bool pageable(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // clear it: an unknown pointer is ordinary host memory
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+// memcpy on `threads` host threads (one below 1 MiB).
+void host_copy(void* dst, const void* src, size_t bytes, int threads) {
+    if (threads <= 1 || bytes < (size_t(1) << 20)) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t per = ((bytes + threads - 1) / threads + 63) & ~size_t(63);
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int t = 0; t < threads; ++t) {
+        const size_t o = std::min(bytes, per * t), e = std::min(bytes, o + per);
+        if (e > o)
+            std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, e - o);
+    }
+}
+
+// `rows` rows of `width` bytes, consecutive in host memory, to the device at pitch dpitch,
+// enqueued on s.  Returns once the host memory has been read (the device copies may still
+// be running), as a copy from pageable memory does.
+cudaError_t upload_rows(HostStaging& H, void* dst, size_t dpitch, const void* src, size_t width,
+                        size_t rows, cudaStream_t s) {
+    if (rows == 0 || width == 0) return cudaSuccess;
+    if (!pageable(src) || width > kStagingBytes)
+        return cudaMemcpy2DAsync(dst, dpitch, src, width, width, rows, cudaMemcpyHostToDevice, s);
+    cudaError_t e = H.init();
+    if (e != cudaSuccess) return e;
+    const size_t per = kStagingBytes / width;  // rows per staging buffer
+    for (size_t r = 0; r < rows; r += per) {
+        const size_t n = std::min(per, rows - r);
+        const int k = H.next;
+        H.next = (k + 1) % kStagingSlots;
+        if ((e = cudaEventSynchronize(H.ev[k])) != cudaSuccess) return e;  // buffer free
+        host_copy(H.buf[k], static_cast<const char*>(src) + r * width, n * width, H.threads);
+        if ((e = cudaMemcpy2DAsync(static_cast<char*>(dst) + r * dpitch, dpitch, H.buf[k], width,
+                                   width, n, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(H.ev[k], s)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t upload(HostStaging& H, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return cudaSuccess;
+    if (!pageable(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    // whole staging buffers as rows, then the remainder
+    const size_t full = bytes / kStagingBytes;
+    cudaError_t e = upload_rows(H, dst, kStagingBytes, src, kStagingBytes, full, s);
+    if (e != cudaSuccess || bytes == full * kStagingBytes) return e;
+    const size_t o = full * kStagingBytes;
+    return upload_rows(H, static_cast<char*>(dst) + o, bytes - o,
+                       static_cast<const char*>(src) + o, bytes - o, 1, s);
+}
+
+// bytes of device memory to the host, after s's earlier work.  To pageable memory: through
+// the staging buffers, returning once the host has every byte; to pinned memory: one copy
+// enqueued on s.
+cudaError_t download(HostStaging& H, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return cudaSuccess;
+    if (!pageable(dst)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = H.init();
+    if (e != cudaSuccess) return e;
+    const size_t n = (bytes + kStagingBytes - 1) / kStagingBytes;
+    auto issue = [&](size_t i) -> cudaError_t {  // device copy of chunk i into buffer i % slots
+        const int k = static_cast<int>(i % kStagingSlots);
+        cudaError_t r = cudaEventSynchronize(H.ev[k]);  // the buffer's last use is over
+        if (r != cudaSuccess) return r;
+        const size_t o = i * kStagingBytes, len = std::min(kStagingBytes, bytes - o);
+        r = cudaMemcpyAsync(H.buf[k], static_cast<const char*>(src) + o, len,
+                            cudaMemcpyDeviceToHost, s);
+        return r != cudaSuccess ? r : cudaEventRecord(H.ev[k], s);
+    };
+    for (size_t i = 0; i < std::min<size_t>(n, kStagingSlots); ++i)
+        if ((e = issue(i)) != cudaSuccess) return e;
+    for (size_t i = 0; i < n; ++i) {
+        const int k = static_cast<int>(i % kStagingSlots);
+        if ((e = cudaEventSynchronize(H.ev[k])) != cudaSuccess) return e;
+        const size_t o = i * kStagingBytes, len = std::min(kStagingBytes, bytes - o);
+        host_copy(static_cast<char*>(dst) + o, H.buf[k], len, H.threads);
+        if (i + kStagingSlots < n && (e = issue(i + kStagingSlots)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 int read_device_error(psm_ctx* c) {
@@ -559,6 +700,7 @@ int psm_destroy(psm_ctx* c) {
         b->release();
     for (cudaEvent_t e : {c->ev_placed, c->ev_staged, c->ev_done[0], c->ev_done[1]})
         if (e) cudaEventDestroy(e);
+    c->staging.release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSM_OK;
@@ -657,9 +799,8 @@ int psm_set_traces(psm_ctx* c, const float* data) {
     if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
     cudaSetDevice(c->device);
     const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
-    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.p, c->ns * sizeof(float), data,
-                                          c->g.n_t * sizeof(float), c->g.n_t * sizeof(float),
-                                          n_tr, cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, upload_rows(c->staging, c->data.p, c->ns * sizeof(float), data,
+                                    c->g.n_t * sizeof(float), n_tr, c->stream));
     if (c->store == psm::kStoreF32)
         PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>(), c->pairs.as<float2>(), n_tr, c->ns,
                                         c->stream));
@@ -716,11 +857,9 @@ int psm_set_traces_segy(psm_ctx* c, const void* records, int64_t n_records, int3
     PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, c->copied, 0));
     for (int64_t r0 = 0; r0 < n_records; r0 += per_chunk) {
         const int64_t n = std::min(per_chunk, n_records - r0);
-        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->seg_rec.as<unsigned char>() + r0 * rec_bytes,
-                                            static_cast<const unsigned char*>(records) +
-                                                r0 * rec_bytes,
-                                            static_cast<size_t>(n) * rec_bytes,
-                                            cudaMemcpyHostToDevice, c->copy_stream));
+        PSM_CUDA_TRY(c->st, upload(c->staging, c->seg_rec.as<unsigned char>() + r0 * rec_bytes,
+                                   static_cast<const unsigned char*>(records) + r0 * rec_bytes,
+                                   static_cast<size_t>(n) * rec_bytes, c->copy_stream));
         PSM_CUDA_TRY(c->st, cudaEventRecord(c->copied, c->copy_stream));
         PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(s, c->copied, 0));
         const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((n + 7) / 8, 148 * 16));
@@ -783,9 +922,8 @@ int psm_get_image_segy(psm_ctx* c, void* out, int32_t format, const int32_t* sou
         c->seg_rec.as<unsigned char>(), c->seg_rec_bytes, c->seg_il.as<int32_t>(),
         c->seg_xl.as<int32_t>(), c->seg_out.as<unsigned char>());
     PSM_CUDA_TRY(c->st, cudaGetLastError());
-    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(out, c->seg_out.p,
-                                        static_cast<size_t>(n_out) * out_rec_bytes,
-                                        cudaMemcpyDeviceToHost, s));
+    PSM_CUDA_TRY(c->st, download(c->staging, out, c->seg_out.p,
+                                 static_cast<size_t>(n_out) * out_rec_bytes, s));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(s));
     return read_device_error(c);
 }
@@ -795,8 +933,7 @@ int psm_get_vrms(psm_ctx* c, float* vrms) {
     if (!c->have_vrms) return c->st.fail(PSM_ERR_STATE, "no Vrms set");
     cudaSetDevice(c->device);
     const size_t n = static_cast<size_t>(c->g.n_il) * c->g.n_xl * c->g.n_t;
-    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(vrms, c->vrms.p, n * sizeof(float),
-                                        cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, download(c->staging, vrms, c->vrms.p, n * sizeof(float), c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     return PSM_OK;
 }
@@ -885,8 +1022,7 @@ int psm_set_vrms(psm_ctx* c, const float* vrms) {
     if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
     cudaSetDevice(c->device);
     const size_t n = static_cast<size_t>(c->g.n_il) * c->g.n_xl * c->g.n_t;
-    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.p, vrms, n * sizeof(float),
-                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, upload(c->staging, c->vrms.p, vrms, n * sizeof(float), c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     c->have_vrms = true;
     return PSM_OK;
@@ -972,8 +1108,7 @@ int psm_get_image(psm_ctx* c, float* image) {
     if (!c->have_geom) return c->st.fail(PSM_ERR_STATE, "psm_set_geometry first");
     cudaSetDevice(c->device);
     const size_t n = static_cast<size_t>(c->g.n_oi) * c->g.n_ox * c->g.n_t;
-    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image, c->image.p, n * sizeof(float),
-                                        cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, download(c->staging, image, c->image.p, n * sizeof(float), c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     return read_device_error(c);
 }
@@ -1101,10 +1236,9 @@ int forward_waves(psm_ctx* c, const float* traces, const float* vrms, float* ima
         const size_t r0 = size_t(lo) * g.n_xl, rows = size_t(hi - lo) * g.n_xl;
         cudaStream_t cs = c->copy_stream;
         if (units[u].first == 0) {
-            PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.as<float>() + r0 * c->ns,
-                                                  c->ns * sizeof(float), traces + lo * per_il,
-                                                  g.n_t * sizeof(float), g.n_t * sizeof(float),
-                                                  rows, cudaMemcpyHostToDevice, cs));
+            PSM_CUDA_TRY(c->st, upload_rows(c->staging, c->data.as<float>() + r0 * c->ns,
+                                            c->ns * sizeof(float), traces + lo * per_il,
+                                            g.n_t * sizeof(float), rows, cs));
             if (c->store == psm::kStoreF32)
                 PSM_CUDA_TRY(c->st, build_pairs(c->data.as<float>() + r0 * c->ns,
                                                 c->pairs.as<float2>() + r0 * c->ns, rows, c->ns,
@@ -1115,9 +1249,8 @@ int forward_waves(psm_ctx* c, const float* traces, const float* vrms, float* ima
                                              c->scales.as<float>() + r0, rows, c->ns, c->store,
                                              cs));
         } else {
-            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->vrms.as<float>() + lo * per_il,
-                                                vrms + lo * per_il, rows * g.n_t * sizeof(float),
-                                                cudaMemcpyHostToDevice, cs));
+            PSM_CUDA_TRY(c->st, upload(c->staging, c->vrms.as<float>() + lo * per_il,
+                                       vrms + lo * per_il, rows * g.n_t * sizeof(float), cs));
         }
         PSM_CUDA_TRY(c->st, cudaEventRecord(ev[u], cs));
         for (; k < chunks.size() && chunk_unit[k] == u; ++k) {  // the waves this upload frees
@@ -1158,10 +1291,9 @@ int forward_waves(psm_ctx* c, const float* traces, const float* vrms, float* ima
         const RowCopy& rc = row_copies[i];
         if (i == 0 || row_copies[i - 1].chunk != rc.chunk)
             PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, ev[n_units + rc.chunk], 0));
-        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + rc.first * row,
-                                            c->image.as<float>() + rc.first * row,
-                                            rc.count * row * sizeof(float),
-                                            cudaMemcpyDeviceToHost, c->d2h_stream));
+        PSM_CUDA_TRY(c->st, download(c->staging, image + rc.first * row,
+                                     c->image.as<float>() + rc.first * row,
+                                     rc.count * row * sizeof(float), c->d2h_stream));
     }
     // the ctx stream's later work follows both compute streams and the uploads
     PSM_CUDA_TRY(c->st, cudaEventRecord(ev_aux, aux_used ? c->aux_stream : c->copy_stream));
@@ -1313,8 +1445,7 @@ int psm_adjoint(psm_ctx* c, const float* image, float* data) {
     PSM_CUDA_TRY(c->st, c->img_in.ensure(n_img * sizeof(float)));
     PSM_CUDA_TRY(c->st, c->cg_q.ensure(n_tr * c->ns * sizeof(float)));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
-    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->img_in.p, image, n_img * sizeof(float),
-                                        cudaMemcpyHostToDevice, c->stream));
+    PSM_CUDA_TRY(c->st, upload(c->staging, c->img_in.p, image, n_img * sizeof(float), c->stream));
     int r = adjoint_dev(c, c->img_in.as<float>(), c->cg_q.as<float>());
     if (r) return r;
     PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(data, c->g.n_t * sizeof(float), c->cg_q.p,
@@ -1357,9 +1488,8 @@ int psm_lsm_cg(psm_ctx* c, const float* data, float* image, int iters, double* r
     double *sc = c->cg_sc.as<double>(), *hist = c->cg_hist.as<double>();
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), s));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(d, 0, nd * sizeof(float), s));
-    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(d, c->ns * sizeof(float), data,
-                                          c->g.n_t * sizeof(float), c->g.n_t * sizeof(float),
-                                          n_tr, cudaMemcpyHostToDevice, s));
+    PSM_CUDA_TRY(c->st, upload_rows(c->staging, d, c->ns * sizeof(float), data,
+                                    c->g.n_t * sizeof(float), n_tr, s));
     PSM_CUDA_TRY(c->st, cudaMemcpyAsync(r, d, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(m, 0, nm * sizeof(float), s));
     PSM_CUDA_TRY(c->st, cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
@@ -1381,7 +1511,7 @@ int psm_lsm_cg(psm_ctx* c, const float* data, float* image, int iters, double* r
         psm::cg_direction_kernel<<<grid_for(nm), 256, 0, s>>>(p, sv, nm, sc);  // p = s + beta p
         PSM_CUDA_TRY(c->st, cudaGetLastError());
     }
-    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image, m, nm * sizeof(float), cudaMemcpyDeviceToHost, s));
+    PSM_CUDA_TRY(c->st, download(c->staging, image, m, nm * sizeof(float), s));
     std::vector<double> h(iters + 1);
     PSM_CUDA_TRY(c->st, cudaMemcpyAsync(h.data(), hist, (iters + 1) * sizeof(double),
                                         cudaMemcpyDeviceToHost, s));
@@ -1608,14 +1738,12 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
             const int kp = keep[k], fresh = fresh_of(k);
             const size_t first = static_cast<size_t>(slabs[k].i0 + kp);
             PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->copy_stream, c->ev_placed, 0));
-            PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->str_tr.p, ns * sizeof(float),
-                                                  traces + first * trace,
-                                                  g->n_t * sizeof(float), g->n_t * sizeof(float),
-                                                  static_cast<size_t>(fresh) * per_il_tr,
-                                                  cudaMemcpyHostToDevice, c->copy_stream));
-            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(c->str_v.p, vrms + first * trace,
-                                                fresh * trace * sizeof(float),
-                                                cudaMemcpyHostToDevice, c->copy_stream));
+            PSM_CUDA_TRY(c->st, upload_rows(c->staging, c->str_tr.p, ns * sizeof(float),
+                                            traces + first * trace, g->n_t * sizeof(float),
+                                            static_cast<size_t>(fresh) * per_il_tr,
+                                            c->copy_stream));
+            PSM_CUDA_TRY(c->st, upload(c->staging, c->str_v.p, vrms + first * trace,
+                                       fresh * trace * sizeof(float), c->copy_stream));
             PSM_CUDA_TRY(c->st, cudaEventRecord(c->ev_staged, c->copy_stream));
         }
         staged = true;  // (nothing new to stage when fresh_of(k) is 0)
@@ -1710,18 +1838,16 @@ int psm_forward_streamed(psm_ctx* c, const psm_geom* g, const int32_t* out_cente
         if (k > 0 && !direct[k - 1]) {
             const psm_slab& pv = slabs[k - 1];
             PSM_CUDA_TRY(c->st, cudaStreamWaitEvent(c->d2h_stream, c->ev_done[(k - 1) & 1], 0));
-            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row,
-                                                c->str_img[(k - 1) & 1].p,
-                                                (pv.o1 - pv.o0) * row * sizeof(float),
-                                                cudaMemcpyDeviceToHost, c->d2h_stream));
+            PSM_CUDA_TRY(c->st, download(c->staging, image + pv.o0 * row,
+                                         c->str_img[(k - 1) & 1].p,
+                                         (pv.o1 - pv.o0) * row * sizeof(float), c->d2h_stream));
             PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->d2h_stream));
         }
     }
     if (n > 0 && !direct[n - 1]) {
         const psm_slab& pv = slabs[n - 1];
-        PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image + pv.o0 * row, c->str_img[(n - 1) & 1].p,
-                                            (pv.o1 - pv.o0) * row * sizeof(float),
-                                            cudaMemcpyDeviceToHost, c->stream));
+        PSM_CUDA_TRY(c->st, download(c->staging, image + pv.o0 * row, c->str_img[(n - 1) & 1].p,
+                                     (pv.o1 - pv.o0) * row * sizeof(float), c->stream));
     }
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->copy_stream));
     return read_device_error(c);
@@ -1950,9 +2076,8 @@ int batch_upload(psm_batch* b) {
     cudaStream_t s = c->stream;
     for (BatchCube& q : b->cubes) {
         const size_t n_tr = static_cast<size_t>(q.n_il) * q.n_xl;
-        PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(q.data.p, q.ns * sizeof(float), q.host,
-                                              q.n_t * sizeof(float), q.n_t * sizeof(float),
-                                              n_tr, cudaMemcpyHostToDevice, s));
+        PSM_CUDA_TRY(c->st, upload_rows(c->staging, q.data.p, q.ns * sizeof(float), q.host,
+                                        q.n_t * sizeof(float), n_tr, s));
         if (b->store == psm::kStoreF32)
             PSM_CUDA_TRY(c->st, build_pairs(q.data.as<float>(), q.pairs.as<float2>(), n_tr,
                                             q.ns, s));
@@ -1963,10 +2088,10 @@ int batch_upload(psm_batch* b) {
     for (BatchProblem& p : b->probs) {
         const psm_geom& g = p.src.geom;
         if (p.src.vrms_kind == PSM_VRMS_CUBE) {
-            PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.vrms.p, p.src.vrms,
-                                                static_cast<size_t>(g.n_il) * g.n_xl * g.n_t *
-                                                    sizeof(float),
-                                                cudaMemcpyHostToDevice, s));
+            PSM_CUDA_TRY(c->st, upload(c->staging, p.vrms.p, p.src.vrms,
+                                       static_cast<size_t>(g.n_il) * g.n_xl * g.n_t *
+                                           sizeof(float),
+                                       s));
         } else if (p.src.vrms_kind == PSM_VRMS_TRACE) {
             PSM_CUDA_TRY(c->st, cudaMemcpyAsync(p.vrms.p, p.src.vrms, g.n_t * sizeof(float),
                                                 cudaMemcpyHostToDevice, s));
@@ -2284,10 +2409,9 @@ int psm_batch_get_image(psm_batch* b, int i, float* image) {
     psm_ctx* c = b->ctx;
     cudaSetDevice(c->device);
     const psm_geom& g = b->probs[i].src.geom;
-    PSM_CUDA_TRY(c->st, cudaMemcpyAsync(image, b->probs[i].image.p,
-                                        static_cast<size_t>(g.n_oi) * g.n_ox * g.n_t *
-                                            sizeof(float),
-                                        cudaMemcpyDeviceToHost, c->stream));
+    PSM_CUDA_TRY(c->st, download(c->staging, image, b->probs[i].image.p,
+                                 static_cast<size_t>(g.n_oi) * g.n_ox * g.n_t * sizeof(float),
+                                 c->stream));
     PSM_CUDA_TRY(c->st, cudaStreamSynchronize(c->stream));
     return read_device_error(c);
 }
