@@ -723,11 +723,15 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
                     eval_pair<AMP, false, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
                                                                    T2[p], F4[p], BB[p], SUM[p]);
             } else {
+                // some lane may fail: a block pair where no lane passes (the aperture grows
+                // with t0, so often the group's shallower pair) is skipped on a warp vote;
+                // its terms would add exact zeros
 #pragma unroll
                 for (int p = PG * gr; p < PG * (gr + 1); ++p)
-                    eval_pair<AMP, true, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc,
-                                                                   scb, T2[p], F4[p], BB[p],
-                                                                   SUM[p]);
+                    if (__any_sync(0xffffffffu, r2 <= fmaxf(BB[p].x, BB[p].y)))
+                        eval_pair<AMP, true, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc,
+                                                                       scb, T2[p], F4[p], BB[p],
+                                                                       SUM[p]);
             }
         }
     }
