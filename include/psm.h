@@ -224,6 +224,18 @@ int psm_adjoint(psm_ctx *ctx, const float *image, float *data);
  * psm_get_traces then reads.  Before the next forward, upload traces again. */
 int psm_adjoint_async(psm_ctx *ctx);
 
+/* The operator pair on caller device memory, enqueued on the ctx stream (psm_stream), with no
+ * host copy and no host synchronisation; psm_synchronize waits and reports device errors.
+ * For iterative solvers that keep their vectors on the device (least-squares migration
+ * sharded over GPUs, where each rank's vectors stay in HBM and only halos cross NVLink).  No
+ * counterpart in the reference.
+ *   psm_forward_device: image[n_oi][n_ox][n_t] = M data[n_il][n_xl][n_t] (fp32 storage;
+ *                       the data become the ctx's resident traces)
+ *   psm_adjoint_device: data[n_il][n_xl][n_t] = M^T image[n_oi][n_ox][n_t] (overwritten)
+ * Both need geometry and vrms. */
+int psm_forward_device(psm_ctx *ctx, const float *d_data, float *d_image);
+int psm_adjoint_device(psm_ctx *ctx, const float *d_image, float *d_data);
+
 /* Least-squares migration: `iters` iterations of CG (CGLS) on min ||M^T m - data||^2 from
  * m = 0, with FP32 operators and FP64 inner products and step lengths computed on the GPU.
  * data [n_il][n_xl][n_t] (host) in, image [n_oi][n_ox][n_t] (host) out, resid[iters + 1]

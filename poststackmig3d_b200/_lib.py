@@ -106,6 +106,8 @@ _CUDA_SYMBOLS = [
     ("psm_set_image", ctypes.c_int, [_P, _P]),
     ("psm_adjoint", ctypes.c_int, [_P, _P, _P]),
     ("psm_adjoint_async", ctypes.c_int, [_P]),
+    ("psm_forward_device", ctypes.c_int, [_P, _P, _P]),
+    ("psm_adjoint_device", ctypes.c_int, [_P, _P, _P]),
     ("psm_lsm_cg", ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P]),
     ("psm_set_variant", ctypes.c_int, [_P, ctypes.c_int]),
     ("psm_get_variant", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),

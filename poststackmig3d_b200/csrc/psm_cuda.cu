@@ -1468,6 +1468,41 @@ int psm_adjoint_async(psm_ctx* c) {
     return PSM_OK;
 }
 
+int psm_forward_device(psm_ctx* c, const float* d_data, float* d_image) {
+    if (!c || !d_data || !d_image) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry and vrms must be set");
+    if (c->store != psm::kStoreF32 || c->g.compensated)
+        return c->st.fail(PSM_ERR_UNSUPPORTED, "device operators take fp32 storage only");
+    cudaSetDevice(c->device);
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    // rows of n_t samples into the fp32 cube's rows of ns (their tails stay zero)
+    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(c->data.p, c->ns * sizeof(float), d_data,
+                                          c->g.n_t * sizeof(float), c->g.n_t * sizeof(float),
+                                          n_tr, cudaMemcpyDeviceToDevice, c->stream));
+    const int r = forward_dev(c, c->data.as<float>(), d_image);
+    if (r) return r;
+    c->have_traces = c->traces_readable = true;
+    return PSM_OK;
+}
+
+int psm_adjoint_device(psm_ctx* c, const float* d_image, float* d_data) {
+    if (!c || !d_image || !d_data) return PSM_ERR_ARG;
+    if (!c->have_geom || !c->have_vrms)
+        return c->st.fail(PSM_ERR_STATE, "geometry and vrms must be set");
+    cudaSetDevice(c->device);
+    const size_t n_tr = static_cast<size_t>(c->g.n_il) * c->g.n_xl;
+    PSM_CUDA_TRY(c->st, c->cg_q.ensure(n_tr * c->ns * sizeof(float)));
+    PSM_CUDA_TRY(c->st, cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    const int r = adjoint_dev(c, d_image, c->cg_q.as<float>());
+    if (r) return r;
+    PSM_CUDA_TRY(c->st, cudaMemcpy2DAsync(d_data, c->g.n_t * sizeof(float), c->cg_q.p,
+                                          c->ns * sizeof(float), c->g.n_t * sizeof(float), n_tr,
+                                          cudaMemcpyDeviceToDevice, c->stream));
+    return PSM_OK;
+}
+
 int psm_lsm_cg(psm_ctx* c, const float* data, float* image, int iters, double* resid) {
     if (!c || !data || !image || iters < 0) return PSM_ERR_ARG;
     if (!c->have_geom || !c->have_vrms)

@@ -425,6 +425,19 @@ class Migrator:
         (psm_adjoint_async); get_traces() reads the result."""
         check(self._L.psm_adjoint_async(self._ctx), self._err)
 
+    def forward_device(self, d_data: int, d_image: int) -> None:
+        """image = M data on device memory (addresses of fp32 arrays [n_il][n_xl][n_t] and
+        [n_oi][n_ox][n_t], e.g. torch tensors' data_ptr()), enqueued on the ctx stream
+        (psm_forward_device); synchronize() waits."""
+        check(self._L.psm_forward_device(self._ctx, ctypes.c_void_p(d_data),
+                                         ctypes.c_void_p(d_image)), self._err)
+
+    def adjoint_device(self, d_image: int, d_data: int) -> None:
+        """data = M^T image on device memory, enqueued on the ctx stream
+        (psm_adjoint_device)."""
+        check(self._L.psm_adjoint_device(self._ctx, ctypes.c_void_p(d_image),
+                                         ctypes.c_void_p(d_data)), self._err)
+
     def lsm_cg(self, data, iters: int):
         """Least-squares migration: CG on min ||M^T m - data||^2 (FP32 operators, FP64
         inner products on the GPU).  Returns (image, data-residual norms [iters + 1])."""

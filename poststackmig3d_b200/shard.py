@@ -10,6 +10,8 @@ output-inline slabs, data vectors are held on each rank's halo of input inlines.
 (spray) of a slab reaches its whole halo, and neighbouring halos overlap, so its contributions
 are summed over the ranks that share an inline (halo_sum, point-to-point), and the CG inner
 products are summed over ranks (each data inline counted once, by its owner).
+lsm_sharded_resident runs the same iteration with every vector in device memory (torch
+tensors, the library's device-pointer operators, halos swapped over NCCL).
 
 The split balances work: the weight of an output inline is its term count when known
 (Migrator.count_terms_rows), else 1.
@@ -259,3 +261,183 @@ def lsm_sharded(g: Geometry, data: np.ndarray, vrms: np.ndarray, rank: int, worl
         if ops is not None and hasattr(ops, "close"):
             ops.close()
     return slabs[rank], m, np.sqrt(np.maximum(np.array(hist), 0.0))
+
+
+# ------------------------------------------------------------ sharded LSM, vectors on the device
+
+
+class _TorchComm:
+    """Exchanges of torch tensors between ranks: device tensors over NCCL, CPU tensors over
+    gloo.  Sums are formed in rank order, so every rank gets the same bits."""
+
+    def __init__(self, rank: int, world: int):
+        self.rank, self.world = rank, world
+
+    def allsum(self, x):
+        """Sum over ranks of a 0-d float64 tensor (stays on its device)."""
+        if self.world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        mine = x.reshape(1)
+        parts = [torch.empty_like(mine) for _ in range(self.world)]
+        dist.all_gather(parts, mine)
+        total = parts[0]
+        for t in parts[1:]:
+            total = total + t
+        return total.reshape(())
+
+    def halo_sum(self, part, halo):
+        """As _Comm.halo_sum, on tensors: each pair of ranks whose halos overlap swaps the
+        overlap point to point (device memory over NCCL: only the halo crosses NVLink)."""
+        if self.world == 1:
+            return part
+        import torch
+        import torch.distributed as dist
+        i0, i1 = halo[self.rank]
+        works, recv = [], {}
+        for s in range(self.world):
+            if s == self.rank:
+                continue
+            a0, a1 = max(i0, halo[s][0]), min(i1, halo[s][1])
+            if a1 <= a0:
+                continue
+            send = part[a0 - i0:a1 - i0].contiguous()
+            buf = torch.empty_like(send)
+            works.append(dist.isend(send, dst=s))
+            works.append(dist.irecv(buf, src=s))
+            recv[s] = (a0, a1, buf)
+        for w in works:
+            w.wait()
+        total = torch.zeros_like(part)
+        for s in range(self.world):
+            if s == self.rank:
+                total += part
+            elif s in recv:
+                a0, a1, buf = recv[s]
+                total[a0 - i0:a1 - i0] += buf
+        return total
+
+
+class _DeviceSlabOps:
+    """Forward and adjoint of one slab on device tensors (psm_forward_device /
+    psm_adjoint_device), enqueued on the library context's stream, which the solver's torch
+    work also runs on."""
+
+    def __init__(self, lg: Geometry, vrms: np.ndarray, device: int):
+        import torch
+        self.m = Migrator(device)
+        self.m.set_geometry(lg)
+        self.m.set_vrms(vrms)
+        self.dev = torch.device(f"cuda:{device}")
+        self.stream = torch.cuda.ExternalStream(self.m.stream_handle(), device=self.dev)
+        self.shape_m = (lg.n_oi, lg.n_ox, lg.n_t)
+        self.shape_d = (lg.n_il, lg.n_xl, lg.n_t)
+
+    def forward(self, d):
+        import torch
+        d = d.contiguous()
+        out = torch.empty(self.shape_m, dtype=torch.float32, device=self.dev)
+        self.m.forward_device(d.data_ptr(), out.data_ptr())
+        return out
+
+    def adjoint(self, rows):
+        import torch
+        rows = rows.contiguous()
+        out = torch.empty(self.shape_d, dtype=torch.float32, device=self.dev)
+        self.m.adjoint_device(rows.data_ptr(), out.data_ptr())
+        return out
+
+    def close(self):
+        self.m.synchronize()  # raises on a device error of the last operators
+        self.m.close()
+
+
+def lsm_sharded_resident(g: Geometry, data: np.ndarray, vrms: np.ndarray, rank: int, world: int,
+                         iters: int, device: Optional[int] = 0, weight=None,
+                         make_ops: Optional[Callable] = None):
+    """lsm_sharded with every vector in device memory: the data residual r and q on this
+    rank's halo of input inlines, the image m, s and p on its slab, all torch tensors on
+    cuda:`device`, and the CG scalars (inner products, alpha, beta) as device scalars, so no
+    iteration waits for the host.  Per iteration each rank runs one adjoint and one forward on
+    its slab (psm_adjoint_device / psm_forward_device on the library's stream, which the torch
+    work shares), swaps the overlap of neighbouring halos point to point and sums three
+    scalars over the ranks; with the nccl backend only those halos and scalars leave the GPU.
+
+    device None runs on CPU tensors (gloo), with `make_ops` (local geometry, halo Vrms, None)
+    -> an object whose forward(halo data) -> rows and adjoint(rows) -> halo data take and return
+    numpy arrays (tests; the oracle stands in for the GPU operators).  Returns (slab, this
+    rank's image rows as a tensor on the solver's device, data-residual norms [iters + 1])."""
+    import contextlib
+    import torch
+    slabs = split_slabs(g, world, weight)
+    owned = owned_ranges(slabs)
+    halo = [(s[2], s[3]) if s[1] > s[0] else (a, a) for s, (a, _) in zip(slabs, owned)]
+    o0, o1 = slabs[rank][0], slabs[rank][1]
+    i0, i1 = halo[rank]
+    a0, a1 = owned[rank]
+    comm = _TorchComm(rank, world)
+    dev = torch.device("cpu") if device is None else torch.device(f"cuda:{device}")
+    shape_d = (i1 - i0, g.n_xl, g.n_t)
+    shape_m = (max(o1 - o0, 0), g.n_ox, g.n_t)
+    ops = None
+    if o1 > o0:
+        lg = slab_geometry(g, slabs[rank])
+        ops = (make_ops or _DeviceSlabOps)(
+            lg, np.ascontiguousarray(vrms[i0:i1], dtype=np.float32), device)
+
+    def fwd(d):
+        if ops is None:
+            return torch.zeros(shape_m, dtype=torch.float32, device=dev)
+        if device is None:
+            return torch.from_numpy(np.asarray(ops.forward(d.numpy()), dtype=np.float32))
+        return ops.forward(d)
+
+    def adj(rows):
+        if ops is None:
+            part = torch.zeros(shape_d, dtype=torch.float32, device=dev)
+        elif device is None:
+            part = torch.from_numpy(np.asarray(ops.adjoint(rows.numpy()), dtype=np.float32))
+        else:
+            part = ops.adjoint(rows)
+        return comm.halo_sum(part, halo)
+
+    def ddot(x, y):  # data space: owned inlines only
+        lo, hi = a0 - i0, a1 - i0
+        return comm.allsum(torch.dot(x[lo:hi].reshape(-1).double(),
+                                     y[lo:hi].reshape(-1).double()))
+
+    def mdot(x, y):
+        return comm.allsum(torch.dot(x.reshape(-1).double(), y.reshape(-1).double()))
+
+    def ratio(a, b):  # a / b, 0 where b is not positive (device scalars)
+        return torch.where(b > 0, a / torch.where(b > 0, b, torch.ones_like(b)),
+                           torch.zeros_like(a))
+
+    stream = getattr(ops, "stream", None) if device is not None else None
+    ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+    try:
+        with ctx:
+            r = torch.from_numpy(np.ascontiguousarray(data[i0:i1], dtype=np.float32)).to(dev)
+            m = torch.zeros(shape_m, dtype=torch.float32, device=dev)
+            hist = [ddot(r, r)]
+            s = fwd(r)
+            p = s.clone()
+            gamma = mdot(s, s)
+            for _ in range(iters):
+                q = adj(p)                                   # q = M^T p
+                delta = ddot(q, q)
+                alpha = ratio(gamma, delta).float()
+                m += alpha * p
+                r -= alpha * q
+                hist.append(ddot(r, r))
+                s = fwd(r)                                   # s = M r
+                gamma_new = mdot(s, s)
+                beta = ratio(gamma_new, gamma).float()
+                gamma = gamma_new
+                p = s + beta * p
+            res = torch.stack(hist).cpu().numpy()
+    finally:
+        if ops is not None and hasattr(ops, "close"):
+            ops.close()
+    return slabs[rank], m, np.sqrt(np.maximum(res, 0.0))

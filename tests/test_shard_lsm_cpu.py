@@ -2,7 +2,9 @@
 gloo ranks each hold a slab of image rows and the halo of data inlines it reads; the spray's
 contributions to shared inlines are summed between neighbours and the CG inner products over
 ranks.  The oracle's forward and adjoint stand in for the GPU operators, so the sharded run
-must follow the single-rank run of the same algorithm to summation-order rounding."""
+must follow the single-rank run of the same algorithm to summation-order rounding.  The
+device-resident form (lsm_sharded_resident: torch tensors, CG scalars kept as tensors) runs
+here on CPU tensors and must follow it too."""
 import os
 import socket
 
@@ -55,7 +57,7 @@ class OracleOps:
                                 lg.d_il, lg.d_xl, lg.amp).astype(np.float32)
 
 
-def _worker(rank, world, port, out_path, weight):
+def _worker(rank, world, port, out_path, weight, resident):
     import sys
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -68,8 +70,14 @@ def _worker(rank, world, port, out_path, weight):
                             timeout=datetime.timedelta(seconds=30))
     try:
         W, g, data = _case()
-        slab, rows, hist = shard.lsm_sharded(g, data, W.vrms_cube(), rank, world, ITERS,
-                                             weight=weight, make_ops=OracleOps)
+        if resident:
+            slab, rows, hist = shard.lsm_sharded_resident(g, data, W.vrms_cube(), rank, world,
+                                                          ITERS, device=None, weight=weight,
+                                                          make_ops=OracleOps)
+            rows = rows.numpy()
+        else:
+            slab, rows, hist = shard.lsm_sharded(g, data, W.vrms_cube(), rank, world, ITERS,
+                                                 weight=weight, make_ops=OracleOps)
         img = shard.gather_rows(g, slab, rows, rank, world, weight)
         np.save(out_path + f".hist{rank}.npy", hist)
         if rank == 0:
@@ -78,11 +86,11 @@ def _worker(rank, world, port, out_path, weight):
         dist.destroy_process_group()
 
 
-def _run(tmp_path, world, weight):
+def _run(tmp_path, world, weight, resident=False):
     out = str(tmp_path / "img.npy")
     ctx = mp.get_context("spawn")
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, out, weight))
+    procs = [ctx.Process(target=_worker, args=(r, world, port, out, weight, resident))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -109,12 +117,24 @@ def test_owned_ranges_partition_the_inlines():
         shard.owned_ranges([(0, 2, 0, 4), (2, 4, 6, 9)])
 
 
+def test_resident_single_rank_follows_host_arrays():
+    from poststackmig3d_b200 import shard
+    W, g, data = _case()
+    rows1, hist1 = _single()
+    slab, rows, hist = shard.lsm_sharded_resident(g, data, W.vrms_cube(), 0, 1, ITERS,
+                                                  device=None, make_ops=OracleOps)
+    assert slab[:2] == (0, g.n_oi)
+    assert np.abs(rows.numpy() - rows1).max() <= 1e-5 * np.abs(rows1).max()
+    np.testing.assert_allclose(hist, hist1, rtol=1e-6)
+
+
+@pytest.mark.parametrize("resident", [False, True])
 @pytest.mark.parametrize("world,skew", [(2, False), (3, True)])
-def test_sharded_lsm_follows_single_rank(tmp_path, world, skew):
+def test_sharded_lsm_follows_single_rank(tmp_path, world, skew, resident):
     W, g, _ = _case()
     # a skewed work split gives uneven slabs and halos that overlap across two neighbours
     weight = np.linspace(1.0, 6.0, g.n_oi) if skew else None
-    out = _run(tmp_path, world, weight)
+    out = _run(tmp_path, world, weight, resident)
     rows1, hist1 = _single()
     img = np.load(out)
     assert img.shape == rows1.shape
