@@ -1145,7 +1145,7 @@ int forward_waves(psm_ctx* c, const float* traces, const float* vrms, float* ima
     // it, and the waves already enqueued migrate meanwhile.  The image rows' copies to the host
     // are enqueued after every upload and launch: into pageable memory such a copy returns only
     // once it is done, which would hold the next upload back until the wave has finished.
-    const int n_blocks = std::min(g.n_il, 8);
+    const int n_blocks = std::min(g.n_il, 16);
     auto block_end = [&](int b) { return static_cast<int>(int64_t(b + 1) * g.n_il / n_blocks); };
     auto block_of = [&](int inl) {  // block holding inline inl
         int b = 0;
