@@ -1328,7 +1328,7 @@ namespace {
 // Samples per adjoint ring stage: 48 KB stages (32 KB for 3 CTAs per SM) of 4-byte fp32 sums
 // or 8-byte fixed-point sums, and at least one whole trace.
 inline int adj_stage_cap(int ns, int minb, int eb) {
-    return std::max((minb == 3 ? 32768 : 49152) / eb, ns);
+    return std::max((minb == 4 ? 20480 : minb == 3 ? 32768 : 49152) / eb, ns);
 }
 
 template <bool AMP, int MINB, bool FIX>
@@ -1374,11 +1374,18 @@ int adjoint_dev(psm_ctx* c, const float* d_rows, float* d_out) {
         PSM_CUDA_TRY(c->st, cudaMemsetAsync(d_out, 0, n_data * sizeof(float), c->stream));
     }
     const int eb = fix ? 8 : 4;
-    // 3 CTAs per SM when their 32 KB stages (and the inline tables) fit a third of the SM
-    A.F.stage_cap = adj_stage_cap(c->ns, 3, eb);
+    // 4 CTAs per SM (fp32 sums) when their 20 KB stages and the inline tables fit a quarter
+    // of the SM, else 3 with 32 KB stages, else 2
+    A.F.stage_cap = adj_stage_cap(c->ns, 4, eb);
     size_t smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap, eb).total;
-    const bool o3 = smem <= 75 * 1024;
-    if (!o3) {
+    const bool o4 = !fix && smem <= 56 * 1024;
+    bool o3 = false;
+    if (!o4) {
+        A.F.stage_cap = adj_stage_cap(c->ns, 3, eb);
+        smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap, eb).total;
+        o3 = smem <= 75 * 1024;
+    }
+    if (!o4 && !o3) {
         A.F.stage_cap = adj_stage_cap(c->ns, 2, eb);
         smem = psm::adj_layout(A.F.max_inl, A.F.stage_cap, eb).total;
     }
@@ -1395,6 +1402,9 @@ int adjoint_dev(psm_ctx* c, const float* d_rows, float* d_out) {
                       : launch_adj<false, 3, true>(A, grid, block, smem, c->stream))
                : (amp ? launch_adj<true, 2, true>(A, grid, block, smem, c->stream)
                       : launch_adj<false, 2, true>(A, grid, block, smem, c->stream));
+    else if (o4)
+        e = amp ? launch_adj<true, 4, false>(A, grid, block, smem, c->stream)
+                : launch_adj<false, 4, false>(A, grid, block, smem, c->stream);
     else
         e = o3 ? (amp ? launch_adj<true, 3, false>(A, grid, block, smem, c->stream)
                       : launch_adj<false, 3, false>(A, grid, block, smem, c->stream))
