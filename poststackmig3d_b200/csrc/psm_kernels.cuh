@@ -722,10 +722,32 @@ __device__ __forceinline__ void visit_slot(const unsigned char* sbase, float r2,
                 for (int p = PG * gr; p < PG * (gr + 1); ++p)
                     eval_pair<AMP, false, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
                                                                    T2[p], F4[p], BB[p], SUM[p]);
-            } else {
+            } else if constexpr (PG == 2) {
                 // some lane may fail: a block pair where no lane passes (the aperture grows
                 // with t0, so often the group's shallower pair) is skipped on a warp vote;
-                // its terms would add exact zeros
+                // its terms would add exact zeros.  Both votes come first, so that when both
+                // block pairs run they share one basic block and their dependency chains
+                // (rsqrt, shared load, interpolation) interleave.
+                const int p0 = PG * gr, p1 = p0 + 1;
+                const bool a0 = __any_sync(0xffffffffu, r2 <= fmaxf(BB[p0].x, BB[p0].y));
+                const bool a1 = __any_sync(0xffffffffu, r2 <= fmaxf(BB[p1].x, BB[p1].y));
+                if (a0 && a1) {
+                    eval_pair<AMP, true, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
+                                                                   T2[p0], F4[p0], BB[p0],
+                                                                   SUM[p0]);
+                    eval_pair<AMP, true, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
+                                                                   T2[p1], F4[p1], BB[p1],
+                                                                   SUM[p1]);
+                } else if (a1) {
+                    eval_pair<AMP, true, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
+                                                                   T2[p1], F4[p1], BB[p1],
+                                                                   SUM[p1]);
+                } else if (a0) {
+                    eval_pair<AMP, true, PACKED, STORE, NT, POFF>(sbase, r2, base, w, sc, scb,
+                                                                   T2[p0], F4[p0], BB[p0],
+                                                                   SUM[p0]);
+                }
+            } else {
 #pragma unroll
                 for (int p = PG * gr; p < PG * (gr + 1); ++p)
                     if (__any_sync(0xffffffffu, r2 <= fmaxf(BB[p].x, BB[p].y)))
