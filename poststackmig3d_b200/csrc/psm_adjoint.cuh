@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(32 * (kTX + 1), MINB) adj_kernel(const AdjPara
                 mv = __ldg(mp + t);
             }
             const PointConst pc = point_const(v, t0v, P.tan2);
-            const float b = pass_bound(pc, P.inv_dt, P.ntm1f);
+            const float b = pass_bound<false>(pc, P.inv_dt, P.ntm1f);
             T2[j] = 1.0f;
             F4[j] = 0.0f;
             MK[j] = 0.0f;
