@@ -13,7 +13,9 @@ mask of the reference, counted exactly by psm_count_terms, per second.
 
 --impl reference times the reference's own CPU implementation of the path
 (MigrationKernel::kirchhoffKernel3DWithPadding compiled from its sources into oracle/_ref,
-OpenMP on all host cores) on a bounded sample of output inlines of the same workload.
+on all host cores, each running the kernel alone on blocks of output crosslines as the
+reference's driver runs it on inlines) on a bounded sample of output inlines of the same
+workload.
 Multi-GPU (torchrun): independent replicas, one per GPU, no collective on the data path
 (weak scaling); value = all ranks' terms / max-over-ranks time.
 """
@@ -219,11 +221,13 @@ def profile_traffic():
 
 
 def cpu_reference_sample(W, g, rows, threads):
-    """Time the reference's own kirchhoffKernel3DWithPadding (oracle/_ref, OpenMP build, all
-    host threads) on output inlines `rows`, with the buffers its driver would prepare
-    (prepareInputBufferWithPadding / prepareVelocitySliceWithPadding).  Falls back to the
-    oracle port when the reference was not built.  Returns (terms, seconds, kind, rows of the
-    image)."""
+    """Time the reference's own kirchhoffKernel3DWithPadding (oracle/_ref) on output inlines
+    `rows`, with the buffers its driver would prepare (prepareInputBufferWithPadding /
+    prepareVelocitySliceWithPadding), on all host threads the way its driver uses them
+    (src/main.cpp:254-256: each thread runs the kernel alone on the next piece of work), a
+    piece being one inline's block of 16 output crosslines (oracle.reference_rows_threaded).
+    Falls back to the oracle port when the reference was not built.  Returns (terms,
+    seconds, kind, rows of the image)."""
     import oracle as O
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     t0 = g.t0()
@@ -239,9 +243,10 @@ def cpu_reference_sample(W, g, rows, threads):
             np.float32(g.dt_seconds), t0, np.float32(g.tan2), g.d_il, g.d_xl, g.amp,
             threads=threads)[0])
     if kind == "reference":
-        out, secs = O.reference_rows(W.data, vr, g.out_center, rows, g.n_ox, g.pad_il,
-                                     g.pad_xl, g.m_il, g.dt_seconds, t0, g.tan2, g.d_il,
-                                     g.d_xl, g.amp, kind="omp")
+        out, secs = O.reference_rows_threaded(W.data, vr, g.out_center, rows, g.n_ox,
+                                              g.pad_il, g.pad_xl, g.m_il, g.dt_seconds, t0,
+                                              g.tan2, g.d_il, g.d_xl, g.amp, threads=threads,
+                                              xl_block=16)
     else:
         out = np.empty((len(rows), g.n_ox, g.n_t), dtype=np.float32)
         secs = 0.0
@@ -285,7 +290,8 @@ def parity_block(W, g, image, rows, ref_rows, threads):
            "reference_fp32_vs_fp64": err(ref_rows, r64) if ref_rows is not None else None,
            "vs_reference": err(got, ref_rows) if ref_rows is not None else None,
            "reference": "kirchhoffKernel3DWithPadding compiled from the reference's sources "
-                        "(oracle/_ref, OpenMP build), same rows and buffers",
+                        "(oracle/_ref, serial build on every host thread), same rows and "
+                        "buffers",
            "fp64": "FP64 oracle of the same operator (oracle/oracle.c, masks in the "
                    "reference's FP32 arithmetic)" + (", fed the dequantised samples"
                                                     if g.precision != "f32" else ""),
@@ -355,7 +361,8 @@ def run_reference(args):
     secs = sum(v[1] for v in vals)
     value = terms / secs / 1e9
     sample = (f"{len(rows)} central output inlines of {W.name} per step "
-              f"(rows {rows[0]}..{rows[-1]}, {terms // max(len(vals), 1)} terms/step)")
+              f"(rows {rows[0]}..{rows[-1]}, {terms // max(len(vals), 1)} terms/step), in "
+              f"blocks of 16 output crosslines taken by {threads} host threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": secs / max(len(vals), 1) * 1e3, "higher_is_better": True,
@@ -524,7 +531,8 @@ def run_ours(args):
         terms, secs, kind, ref_rows = cpu_reference_sample(W, g, rows, threads)
         cpu = {"value": terms / secs / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{len(rows)} central output inlines of {W.name} "
-                         f"({terms} terms, {secs:.1f} s)"}
+                         f"({terms} terms, {secs:.1f} s), in blocks of 16 output "
+                         f"crosslines taken by {threads} host threads"}
         if kind == "reference":
             image = m.get_image()
             parity = parity_block(W, g, image, rows, ref_rows, threads)

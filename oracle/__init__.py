@@ -278,6 +278,55 @@ def reference_rows(data, vrms, out_center, rows, n_ox, pad_il, pad_xl, m_il, dt,
     return out, secs
 
 
+def reference_rows_threaded(data, vrms, out_center, rows, n_ox, pad_il, pad_xl, m_il, dt, t0,
+                            tan2, d_il, d_xl, amp=True, threads=1, xl_block=16):
+    """reference_rows with the work spread over `threads` host threads the way the
+    reference's driver spreads it (src/main.cpp:254-256): every thread runs the kernel alone on
+    a piece of work it takes when it is free.  A piece here is one output inline's block of
+    `xl_block` output crosslines, given to the reference's serial build as current_xl_start
+    and a shorter output slice; the kernel computes every output crossline on its own
+    (src/migration_kernel.cpp:75-375), so the rows equal the whole-inline calls.  (The
+    kernel's own OpenMP loop splits one inline's crosslines statically, and the crosslines
+    near the cube's edges hold fewer terms, which leaves threads idle.)  Returns (image rows
+    [len(rows)][n_ox][n_t] float32, wall seconds of the kernel calls)."""
+    import time
+    from concurrent.futures import ThreadPoolExecutor
+    n_il, n_xl, n_t = data.shape
+    L = ref_lib("serial")
+    out = np.zeros((len(rows), n_ox, n_t), dtype=np.float32)
+    t0 = np.ascontiguousarray(t0, dtype=np.float32)
+    jobs = []
+    for r in rows:  # the buffers the driver prepares (reference_rows), outside the timing
+        c = int(out_center[r])
+        rs, re = max(0, c - m_il), min(n_il, c + m_il + 1)
+        il0, il1 = max(0, rs - pad_il), min(n_il, re + pad_il)
+        nbx = n_xl + 2 * pad_xl
+        if pad_xl:
+            buf = np.zeros((il1 - il0, nbx, n_t), dtype=np.float32)
+            buf[:, pad_xl:pad_xl + n_xl] = data[il0:il1]
+            vel = np.zeros((nbx, n_t), dtype=np.float32)
+            vel[pad_xl:pad_xl + n_xl] = vrms[c]
+        else:
+            buf = np.ascontiguousarray(data[il0:il1], dtype=np.float32)
+            vel = np.ascontiguousarray(vrms[c], dtype=np.float32)
+        jobs.append((buf, vel, np.arange(il0, il1, dtype=np.int32), c - il0))
+    units = [(k, x0, min(xl_block, n_ox - x0)) for x0 in range(0, n_ox, xl_block)
+             for k in range(len(rows))]
+
+    def run(u):
+        k, x0, nb = u
+        buf, vel, il_pos, cur = jobs[k]
+        L.ref_kirchhoff_inline(buf, buf.shape[0], buf.shape[1], n_t, vel, out[k, x0:x0 + nb],
+                               nb, il_pos, cur, x0, np.float32(dt), t0, np.float32(tan2),
+                               np.float32(d_il), np.float32(d_xl), int(bool(amp)))
+
+    with ThreadPoolExecutor(max_workers=max(1, int(threads))) as ex:
+        t = time.perf_counter()
+        list(ex.map(run, units))
+        secs = time.perf_counter() - t
+    return out, secs
+
+
 def write_config(path: str, **kv) -> None:
     with open(path, "w") as f:
         for k, v in kv.items():

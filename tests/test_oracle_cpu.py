@@ -108,3 +108,22 @@ def test_adjoint_oracle_dot_product():
     lhs = float(np.sum(Ld * m))
     rhs = float(np.sum(d.astype(np.float64) * Ltm))
     assert abs(lhs - rhs) <= 1e-10 * max(abs(lhs), 1.0)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="the reference was not built (oracle/_ref)")
+@pytest.mark.parametrize("pad", [0, 3])
+def test_reference_rows_threaded_equal_whole_inline_calls(pad):
+    """The CPU baseline's threaded form of the reference kernel (blocks of output crosslines
+    on host threads, each through the reference's serial build) gives the rows of the
+    whole-inline calls of the same build bit for bit."""
+    W = S.random_workload(61, 14, 23, 120, vel_kind="lateral", pad_il=pad, pad_xl=pad)
+    vr = W.vrms_cube()
+    g = plan_geometry(14, 23, 120, W.dt, W.d_il, W.d_xl, W.angle, float(vr.max()), pad, pad,
+                      True)
+    rows = [0, g.n_oi // 2, g.n_oi - 1]
+    args = (W.data, vr, g.out_center, rows, g.n_ox, g.pad_il, g.pad_xl, g.m_il, g.dt_seconds,
+            g.t0(), g.tan2, g.d_il, g.d_xl, True)
+    whole, _ = O.reference_rows(*args, kind="serial")
+    threaded, secs = O.reference_rows_threaded(*args, threads=4, xl_block=5)
+    assert secs >= 0.0
+    assert np.array_equal(threaded, whole)
