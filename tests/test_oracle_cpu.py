@@ -71,7 +71,8 @@ def test_oracle_reproduces_reference_outputs(tmp_path, name):
 
 
 def test_oracle_counts_config1():
-    """Config 1 term count of the survey's replica of the reference masks."""
+    """Config 1 term count: the reference masks applied to real traces (an independent
+    replica of the masks counted 2,855,016,288 terms with the zero padding traces too)."""
     W = S.workload_config1()
     t0 = O.t0_times(501, 0.002)
     tan2 = O.tan2_theta(30.0)
